@@ -1,0 +1,417 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 line-of-sight integrator.
+
+Workload (default): Nside 128/256/512/1024 over 4 shells
+to 30 kpc with 0.01 kpc radial steps (21.6 G LOS samples per frequency),
+512^3 FP32 random-field grids (B_rnd 3 components + lognormal n_e) on a
+40 x 40 x 10 kpc box plus the analytic spiral B_reg and CRE_ana, three
+frequencies 0.408 / 1.4 / 30 GHz in the reference's Pipeline order (the
+first pass also produces DM and FD).  One step = the three frequency passes.
+
+Reported: LOS samples/s of the FP32-compensated form (value, inputs resident
+in HBM), ms per Nside-1024 map, the plain-FP64 GPU form on the same inputs,
+the FP32C-vs-FP64 map errors, an end-to-end number through the host-buffer
+C ABI (grid upload + maps download inside the timed region), the roofline of
+the shell-integration kernel, and the reference CPU integrator timed on a
+bounded sample on this host's cores.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LOS samples/s & ms per Nside-1024 map (FP32-comp vs FP64 GPU), adjoint/fwd ratio"
+UNIT = "LOS samples/s"
+BYTES_PER_SAMPLE = {"fp32c": 128, "fp64": 256}  # 8 corners x 4 gridded components
+
+WORKLOADS = {
+    "config3": dict(nside_shells=[128, 256, 512, 1024], r_max_kpc=30.0, res_kpc=0.01,
+                    freqs_ghz=[0.408, 1.4, 30.0], grid_n=512, seeds=(3, 4),
+                    cpu_sample_shells=[8, 16, 32, 64]),
+    "small": dict(nside_shells=[32, 64, 128, 256], r_max_kpc=30.0, res_kpc=0.01,
+                  freqs_ghz=[0.408, 1.4, 30.0], grid_n=128, seeds=(3, 4),
+                  cpu_sample_shells=[4, 8, 16, 32]),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_sample(name):
+    """Bytes of DRAM traffic per LOS sample of the integration kernel from
+    the committed ncu summary (profiles/<name>), or None."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_sample:"):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def setup_dist(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def make_passes(wl, nside_shells=None):
+    from hammurabix_b200 import workloads as W
+    return W.config_grid(nside_shells or wl["nside_shells"], wl["r_max_kpc"], wl["res_kpc"],
+                         wl["freqs_ghz"])
+
+
+def cpu_baseline(wl, host_fields, steps=1):
+    """The reference's FP64 OpenMP integrator (oracle/_ref, compiled from the
+    reference sources) on a bounded sample: the workload's geometry, grids and
+    first frequency pass at 1/16 of its angular resolution, all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from hammurabix_b200 import workloads as W
+    ref = pyoracle.Reference()
+    threads = os.cpu_count()
+    o = make_passes(wl, wl["cpu_sample_shells"])[0]
+    n = wl["grid_n"]
+    grids = W.grids_dict(n, *host_fields)
+    m = W.grid_models()
+    samples = W.samples_of(o)
+    times = []
+    for _ in range(steps):
+        _, secs = ref.write_grid(o, m, grids, nthreads=threads)
+        times.append(secs)
+    return {"samples": samples, "seconds": times, "threads": threads,
+            "sample": (f"pass 1 ({o.sync_freq / 1e9:g} GHz with DM+FD) of the workload at "
+                       f"Nside {'/'.join(str(s) for s in wl['cpu_sample_shells'])}, "
+                       f"same {n}^3 grids, {samples} LOS samples; Integrator::write_grid only")}
+
+
+def run_reference_arm(args, wl):
+    ws, rank, _ = setup_dist(args)
+    if rank != 0:
+        return
+    import numpy as np
+    from hammurabix_b200 import workloads as W
+    b = W.random_grids_torch(wl["grid_n"], *wl["seeds"], device="cpu")
+    host = [t.double().numpy().reshape(-1) for t in b]
+    del b
+    cb = cpu_baseline(wl, host, steps=args.warmup + args.steps)
+    secs = cb["seconds"][args.warmup:]
+    t = sum(secs) / len(secs)
+    value = cb["samples"] / t
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": args.workload + " (bounded sample)",
+                                        "sample": cb["sample"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cb["threads"],
+                         "kind": "reference", "sample": cb["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def rel_err(a, b):
+    d = (a - b).abs().max().item()
+    s = b.abs().max().item()
+    return d / s if s > 0 else d
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="config3", choices=sorted(WORKLOADS))
+    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference_arm(args, wl)
+
+    import numpy as np
+    import torch
+    from hammurabix_b200 import abi, workloads as W
+    from hammurabix_b200.integrator import Integrator
+
+    ws, rank, local = setup_dist(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    n = wl["grid_n"]
+    t0 = time.time()
+    fields = W.random_grids_torch(n, *wl["seeds"], device=dev)
+    f64 = [t.double().reshape(-1).contiguous() for t in fields]
+    del fields
+    log(f"[rank {rank}] grids {n}^3 generated in {time.time() - t0:.1f}s")
+    desc = W.grid_desc(n)
+    models = W.grid_models()
+    passes = make_passes(wl)
+    samples_step = sum(W.samples_of(o) for o in passes)
+    nout = max(wl["nside_shells"])
+    npx = abi.npix(nout)
+
+    def outputs():
+        return [torch.zeros(npx, dtype=torch.float64, device=dev) for _ in range(5)]
+
+    def make_integ(prec):
+        ig = Integrator(prec, device=local)
+        ig.set_stream(stream.cuda_stream)
+        ig.set_models(models)
+        ig.upload_grid_device(abi.HXG_FIELD_BRND, desc, f64[:3])
+        ig.upload_grid_device(abi.HXG_FIELD_TEREG, desc, f64[3:])
+        return ig
+
+    def step(ig, outs):
+        for o in passes:
+            ig.write_grid_device(o, outs[0] if o.do_dm else None, outs[1] if o.do_fd else None,
+                                 outs[2], outs[3], outs[4])
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if ws > 1:
+            torch.distributed.barrier()
+
+    def timed(ig, outs, k):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        ev0.record(stream)
+        for _ in range(k):
+            step(ig, outs)
+        ev1.record(stream)
+        barrier()
+        return ev0.elapsed_time(ev1) / 1e3
+
+    def max_over_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return t.item()
+
+    # ---- FP32-compensated form: the product path ------------------------
+    ig32 = make_integ("fp32c")
+    out32 = outputs()
+    for _ in range(args.warmup):
+        step(ig32, out32)
+    ig32.set_timing(True)
+    lc0 = ig32.launch_count()
+    with ClockSampler(local) as clk:
+        t32 = max_over_ranks(timed(ig32, out32, args.steps))
+    launches = ig32.launch_count() - lc0
+    kms, klaunch, ksamples = ig32.get_timing()
+    ig32.set_timing(False)
+    value = ws * samples_step * args.steps / t32
+    ms_step = t32 / args.steps * 1e3
+    log(f"[rank {rank}] fp32c: {ms_step:.1f} ms/step, {value:.4g} samples/s")
+
+    # ---- plain FP64 GPU form on the same inputs ----------------------------
+    fp64 = None
+    errs = None
+    if args.fp64_steps > 0:
+        ig64 = make_integ("fp64")
+        out64 = outputs()
+        step(ig64, out64)
+        t64 = max_over_ranks(timed(ig64, out64, args.fp64_steps))
+        ms64 = t64 / args.fp64_steps * 1e3
+        fp64 = {"ms_per_step": ms64, "ms_per_map": ms64 / len(passes),
+                "samples_per_s": ws * samples_step / (ms64 / 1e3)}
+        # errors of the last pass (0.408 GHz, sync only) and of the first
+        # pass's DM/FD: rerun pass 0 and the last pass in both forms
+        errs = {}
+        for idx in (0, len(passes) - 1):
+            o = passes[idx]
+            a, b = outputs(), outputs()
+            ig32.write_grid_device(o, a[0] if o.do_dm else None, a[1] if o.do_fd else None,
+                                   a[2], a[3], a[4])
+            ig64.write_grid_device(o, b[0] if o.do_dm else None, b[1] if o.do_fd else None,
+                                   b[2], b[3], b[4])
+            torch.cuda.synchronize(dev)
+            tag = f"{o.sync_freq / 1e9:g}GHz"
+            for j, k in enumerate(("dm", "fd", "I", "Q", "U")):
+                if (j == 0 and not o.do_dm) or (j == 1 and not o.do_fd):
+                    continue
+                errs[f"{k}@{tag}" if j >= 2 else k] = rel_err(a[j], b[j])
+        ig64.close()
+        del out64
+        log(f"[rank {rank}] fp64: {ms64:.1f} ms/step; errors {errs}")
+
+    # ---- end to end through the host-buffer C ABI -----------------------------
+    e2e = None
+    if args.e2e_steps > 0:
+        pinned = [torch.empty(t.numel(), dtype=torch.float64, pin_memory=True) for t in f64]
+        for p, t in zip(pinned, f64):
+            p.copy_(t)
+        hosts = [p.numpy() for p in pinned]
+        outs_h = [np.zeros(npx) for _ in range(5)]
+        ige = Integrator("fp32c", device=local)
+        ige.set_models(models)
+
+        def e2e_step():
+            ige.upload_grid(abi.HXG_FIELD_BRND, desc, hosts[:3])
+            ige.upload_grid(abi.HXG_FIELD_TEREG, desc, hosts[3:])
+            for o in passes:
+                res = ige.write_grid(o)
+                for j, k in enumerate(("dm", "fd", "is", "qs", "us")):
+                    if res[k] is not None:
+                        outs_h[j] = res[k]
+
+        e2e_step()
+        barrier()
+        te0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        barrier()
+        te = max_over_ranks((time.perf_counter() - te0) / args.e2e_steps)
+        h2d = sum(h.nbytes for h in hosts)
+        d2h = sum(8 * (abi.npix(o.nside_dm) * o.do_dm + abi.npix(o.nside_fd) * o.do_fd
+                       + 3 * abi.npix(o.nside_sync)) for o in passes)
+        e2e = {"value": ws * samples_step / te, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": te * 1e3}
+        ige.close()
+        del pinned, hosts
+        log(f"[rank {rank}] e2e: {te * 1e3:.1f} ms/step")
+
+    # ---- roofline of the shell-integration kernel -------------------------------
+    peak, peak_kind = measured_peaks()
+    per_launch_s = kms / 1e3 / max(klaunch, 1)
+    samples_per_launch = ksamples / max(klaunch, 1)
+    achieved = samples_per_launch * BYTES_PER_SAMPLE["fp32c"] / per_launch_s / 1e9
+    tps = traffic_per_sample("shell_fp32c_config3.md")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": (tps * samples_per_launch) if tps else None,
+                "kernel": "hxg::shell_fp32c_kernel<1,true>",
+                "kernel_share_of_step": (kms / 1e3) / t32 if t32 > 0 else None,
+                "kernel_samples_per_s": ksamples / (kms / 1e3) if kms > 0 else None}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        host = [t.cpu().numpy() for t in f64]
+        cb = cpu_baseline(wl, host)
+        v = cb["samples"] / cb["seconds"][0]
+        cpu = {"value": v, "unit": UNIT, "cores": cb["threads"], "kind": "reference",
+               "sample": cb["sample"]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32c",
+            "data": "synthetic",
+            "config": {"workload": f"{args.workload}: Nside "
+                       f"{'/'.join(str(s) for s in wl['nside_shells'])} x "
+                       f"{len(wl['nside_shells'])} shells to {wl['r_max_kpc']:g} kpc, "
+                       f"{wl['res_kpc']} kpc steps, {n}^3 FP32 grids, "
+                       f"{'/'.join(str(f) for f in wl['freqs_ghz'])} GHz",
+                       "samples_per_step": samples_step, "passes_per_step": len(passes),
+                       "l2": "inputs larger than L2 (grids "
+                             f"{4 * 4 * n ** 3 / 1e9:.2f} GB FP32)",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+            "ms_per_map": ms_step / len(passes),
+            "fp64": fp64,
+            "fp32c_speedup_vs_fp64": (fp64["ms_per_step"] / ms_step) if fp64 else None,
+            "fp32c_max_rel_err_vs_fp64": errs,
+            "adjoint_fwd_ratio": None,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ig32.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,994 @@
+// hxg_api.cu -- host glue of the C ABI (include/hxg.h): the B200
+// replacement of Integrator::write_grid (source/integrator/integrator.cc:23-134).
+//
+// The shell loop, shell geometry, mask duplication and all per-launch
+// constants run here in FP64 on the host; the per-pixel radial integration
+// (hxg_integrate.cuh) and the shell merge (hxg_kernels.cu) run on the GPU.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/hxg.h"
+#include "hxg_integrate.cuh"
+#include "hxg_internal.h"
+
+using namespace hxg;
+
+namespace {
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+struct Slot {
+  bool present = false;
+  hxg_grid_desc_t desc{};
+  double *d[3] = {nullptr, nullptr, nullptr};
+  size_t n = 0;
+};
+
+struct Group {
+  hxg_grid_desc_t desc{};
+  int b_slots[2] = {-1, -1};
+  int t_slots[2] = {-1, -1};
+  void *rec = nullptr;
+  size_t n = 0;
+};
+
+}  // namespace
+
+struct hxg_handle {
+  int device = 0;
+  int precision = HXG_FP64;
+  int sm_count = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  hxg_models_t models{};
+  bool have_models = false;
+  Slot slots[5];
+  std::vector<Group> groups;
+  bool groups_dirty = true;
+  bool have_mask = false;
+  uint32_t mask_nside = 0;
+  std::vector<double> mask_host;
+  std::map<uint32_t, unsigned char *> mask_dev;
+  DevBuf tmp[5];
+  DevBuf out[5];
+  bool timing = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+  std::vector<int64_t> event_samples;
+  double acc_ms = 0.;
+  int64_t acc_launches = 0, acc_samples = 0;
+  double waves = 4.0;
+  int64_t launch_count = 0;
+};
+
+namespace {
+
+int fail(hxg_handle *h, int code, const char *fmt, ...) {
+  if (h) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    h->err = buf;
+  }
+  return code;
+}
+
+int cuda_fail(hxg_handle *h, cudaError_t e, const char *what) {
+  if (e == cudaErrorMemoryAllocation)
+    return fail(h, HXG_ERR_OOM, "%s: %s", what, cudaGetErrorString(e));
+  return fail(h, HXG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define HXG_CK(call)                                       \
+  do {                                                     \
+    cudaError_t e_ = (call);                               \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+  } while (0)
+
+int ensure(hxg_handle *h, DevBuf &b, size_t bytes) {
+  if (b.bytes >= bytes) return HXG_OK;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc");
+  b.bytes = bytes;
+  return HXG_OK;
+}
+
+bool is_pow2(uint32_t n) { return n > 0 && (n & (n - 1)) == 0; }
+
+uint64_t npix_of(uint32_t nside) { return 12ull * nside * nside; }
+
+bool same_geometry(const hxg_grid_desc_t &a, const hxg_grid_desc_t &b) {
+  return a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && a.x_min == b.x_min &&
+         a.x_max == b.x_max && a.y_min == b.y_min && a.y_max == b.y_max &&
+         a.z_min == b.z_min && a.z_max == b.z_max;
+}
+
+bool models_supported(const hxg_models_t &m, std::string *why) {
+  switch (m.breg) {
+    case HXG_BREG_NONE: case HXG_BREG_GRID: case HXG_BREG_LSA:
+    case HXG_BREG_UNIF: case HXG_BREG_CART: case HXG_BREG_HELIX:
+    case HXG_BREG_SPIRAL:
+      break;
+    default:
+      *why = "regular B model not supported on the device";
+      return false;
+  }
+  if (m.brnd != HXG_BRND_NONE && m.brnd != HXG_BRND_GRID) {
+    *why = "random B model must be NONE or GRID";
+    return false;
+  }
+  switch (m.tereg) {
+    case HXG_TEREG_NONE: case HXG_TEREG_GRID: case HXG_TEREG_UNIF:
+    case HXG_TEREG_EXPDISK:
+      break;
+    default:
+      *why = "regular n_e model not supported on the device";
+      return false;
+  }
+  if (m.ternd != HXG_TERND_NONE && m.ternd != HXG_TERND_GRID) {
+    *why = "random n_e model must be NONE or GRID";
+    return false;
+  }
+  if (m.cre != HXG_CRE_NONE && m.cre != HXG_CRE_ANA && m.cre != HXG_CRE_UNIF) {
+    *why = "CRE model not supported on the device";
+    return false;
+  }
+  return true;
+}
+
+// The slots whose grids the models read (Breg/Brnd/TEreg/TErnd::read_field,
+// breg.cc:11-26, brnd.cc:12-23, tereg.cc:11-25, ternd.cc:12-19).
+void active_slots(const hxg_models_t &m, bool act[4]) {
+  act[HXG_FIELD_BREG] = m.breg == HXG_BREG_GRID;
+  act[HXG_FIELD_BRND] = m.brnd == HXG_BRND_GRID;
+  act[HXG_FIELD_TEREG] = m.tereg == HXG_TEREG_GRID;
+  act[HXG_FIELD_TERND] = m.ternd == HXG_TERND_GRID;
+}
+
+void free_groups(hxg_handle *h) {
+  for (auto &g : h->groups)
+    if (g.rec) cudaFree(g.rec);
+  h->groups.clear();
+}
+
+// Pack every active grid slot into per-geometry 4-component record arrays.
+int build_groups(hxg_handle *h) {
+  if (!h->groups_dirty) return HXG_OK;
+  free_groups(h);
+  bool act[4];
+  active_slots(h->models, act);
+  for (int s = 0; s < 4; ++s) {
+    if (!act[s]) continue;
+    if (!h->slots[s].present)
+      return fail(h, HXG_ERR_STATE, "model reads grid slot %d but no grid was uploaded", s);
+    Group *grp = nullptr;
+    for (auto &g : h->groups)
+      if (same_geometry(g.desc, h->slots[s].desc)) grp = &g;
+    if (!grp) {
+      h->groups.emplace_back();
+      grp = &h->groups.back();
+      grp->desc = h->slots[s].desc;
+      grp->n = h->slots[s].n;
+    }
+    const bool is_b = (s == HXG_FIELD_BREG || s == HXG_FIELD_BRND);
+    int *list = is_b ? grp->b_slots : grp->t_slots;
+    if (list[0] < 0)
+      list[0] = s;
+    else
+      list[1] = s;
+  }
+  if (h->groups.size() > (size_t)kMaxGroups)
+    return fail(h, HXG_ERR_UNSUPPORTED, "more than %d grid geometries", kMaxGroups);
+  const bool fp32 = h->precision == HXG_FP32C;
+  const size_t esz = fp32 ? sizeof(float) : sizeof(double);
+  for (auto &g : h->groups) {
+    cudaError_t e = cudaMalloc(&g.rec, g.n * 4 * esz);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc(grid records)");
+    const double *b0[3] = {nullptr, nullptr, nullptr};
+    const double *b1[3] = {nullptr, nullptr, nullptr};
+    if (g.b_slots[0] >= 0)
+      for (int k = 0; k < 3; ++k) b0[k] = h->slots[g.b_slots[0]].d[k];
+    if (g.b_slots[1] >= 0)
+      for (int k = 0; k < 3; ++k) b1[k] = h->slots[g.b_slots[1]].d[k];
+    const double *t0 = g.t_slots[0] >= 0 ? h->slots[g.t_slots[0]].d[0] : nullptr;
+    const double *t1 = g.t_slots[1] >= 0 ? h->slots[g.t_slots[1]].d[0] : nullptr;
+    const double bscale = fp32 ? 1.0 / cgs::muGauss : 1.0;
+    HXG_CK(launch_pack(h->stream, fp32, g.n, g.rec, b0, b1, t0, t1, bscale, 1.0));
+    ++h->launch_count;
+  }
+  h->groups_dirty = false;
+  return HXG_OK;
+}
+
+// Hampisk::duplicate (include/hamsk.h:55-103).
+void mask_duplicate_host(uint32_t pivot_nside, const double *pm,
+                         uint32_t nside, double *out) {
+  const Hpx hp = hpx_make(pivot_nside), ht = hpx_make(nside);
+  if (pivot_nside == nside) {
+    std::memcpy(out, pm, sizeof(double) * hp.npix);
+    return;
+  }
+  for (uint64_t i = 0; i < ht.npix; ++i) out[i] = 0.;
+  if (pivot_nside > nside) {
+    const uint64_t fact = pivot_nside / nside;
+    for (uint64_t m = 0; m < ht.npix; ++m) {
+      int64_t x, y, f;
+      hpx_ring2xyf(ht, m, x, y, f);
+      bool hit = false;
+      for (uint64_t j = fact * (uint64_t)y; j < fact * (uint64_t)(y + 1) && !hit; ++j)
+        for (uint64_t i = fact * (uint64_t)x; i < fact * (uint64_t)(x + 1); ++i) {
+          hit = pm[hpx_xyf2ring(hp, (int64_t)i, (int64_t)j, f)] > 0;
+          if (hit) break;
+        }
+      out[m] = (double)hit;
+    }
+  } else {
+    const uint64_t fact = nside / pivot_nside;
+    for (uint64_t m = 0; m < hp.npix; ++m) {
+      const double val = pm[m];
+      int64_t x, y, f;
+      hpx_ring2xyf(hp, m, x, y, f);
+      for (uint64_t j = fact * (uint64_t)y; j < fact * (uint64_t)(y + 1); ++j)
+        for (uint64_t i = fact * (uint64_t)x; i < fact * (uint64_t)(x + 1); ++i)
+          out[hpx_xyf2ring(ht, (int64_t)i, (int64_t)j, f)] = val;
+    }
+  }
+}
+
+int device_mask(hxg_handle *h, uint32_t nside, const unsigned char **out) {
+  auto it = h->mask_dev.find(nside);
+  if (it != h->mask_dev.end()) {
+    *out = it->second;
+    return HXG_OK;
+  }
+  const uint64_t n = npix_of(nside);
+  std::vector<double> dup(n);
+  mask_duplicate_host(h->mask_nside, h->mask_host.data(), nside, dup.data());
+  std::vector<unsigned char> flags(n);
+  for (uint64_t i = 0; i < n; ++i) flags[i] = dup[i] == 1.0 ? 1 : 0;
+  unsigned char *d = nullptr;
+  HXG_CK(cudaMalloc(&d, n));
+  HXG_CK(cudaMemcpyAsync(d, flags.data(), n, cudaMemcpyHostToDevice, h->stream));
+  HXG_CK(cudaStreamSynchronize(h->stream));
+  h->mask_dev[nside] = d;
+  *out = d;
+  return HXG_OK;
+}
+
+void clear_masks(hxg_handle *h) {
+  for (auto &kv : h->mask_dev) cudaFree(kv.second);
+  h->mask_dev.clear();
+}
+
+// Integrator::assemble_shell_ref (integrator.cc:231-254)
+void shell_ref(const hxg_obs_t &o, uint32_t s, double &d_start,
+               double &delta_d, uint64_t &step) {
+  const double ds = o.radii_shell[s], de = o.radii_shell[s + 1];
+  double dd = o.oc_r_res;
+  step = (uint64_t)std::floor((de / dd - ds / dd));
+  dd = (de - ds) / (double)step;
+  d_start = ds;
+  delta_d = dd;
+}
+
+// CRE spectral index at the observer (cre_ana.cc:114-119, cre_unif.cc:175-178)
+double cre_index_at(const hxg_models_t &m, const double p[3]) {
+  if (m.cre == HXG_CRE_ANA) {
+    const double r = std::sqrt(p[0] * p[0] + p[1] * p[1]) / cgs::kpc;
+    const double z = std::fabs(p[2]) / cgs::kpc;
+    return -m.cre_ana.alpha + m.cre_ana.beta * r + m.cre_ana.theta * z;
+  }
+  return -(m.cre_unif.alpha);
+}
+
+// Fill the model block in the working units of the form: CGS for FP64,
+// kpc / muGauss for FP32C (L = length scale, Bu = field scale).
+DevModels dev_models(const hxg_models_t &m, const double obs[3], double L,
+                     double Bu) {
+  DevModels d{};
+  d.breg = m.breg == HXG_BREG_GRID ? kBregNone : m.breg;
+  d.tereg = m.tereg == HXG_TEREG_GRID ? kTeregNone : m.tereg;
+  d.cre = m.cre;
+  d.cre_const_index =
+      (m.cre == HXG_CRE_UNIF) ||
+      (m.cre == HXG_CRE_ANA && m.cre_ana.beta == 0. && m.cre_ana.theta == 0.);
+  d.kpc = cgs::kpc * L;
+  for (int i = 0; i < 3; ++i) d.obs[i] = obs[i] * L;
+  d.lsa_b0 = m.lsa.b0 * Bu;
+  d.lsa_psi0 = m.lsa.psi0;
+  d.lsa_psi1 = m.lsa.psi1;
+  d.lsa_chi0 = m.lsa.chi0;
+  if (m.breg == HXG_BREG_UNIF) {
+    d.const_b[0] = m.unif.bp * std::cos(m.unif.l0) * Bu;
+    d.const_b[1] = m.unif.bp * std::sin(m.unif.l0) * Bu;
+    d.const_b[2] = m.unif.bv * Bu;
+  } else if (m.breg == HXG_BREG_CART) {
+    d.const_b[0] = m.cart.bx * Bu;
+    d.const_b[1] = m.cart.by * Bu;
+    d.const_b[2] = m.cart.bz * Bu;
+  }
+  d.hx_bx = m.helix.bx * Bu;
+  d.hx_by = m.helix.by * Bu;
+  d.hx_bz = m.helix.bz * Bu;
+  d.hx_rmin = m.helix.r_min * L;
+  d.hx_rmax = m.helix.r_max * L;
+  const double rsun = std::sqrt(obs[0] * obs[0] + obs[1] * obs[1]);
+  d.sp_b0 = m.spiral.b0 * Bu;
+  d.sp_sin = std::sin(m.spiral.pitch);
+  d.sp_cos = std::cos(m.spiral.pitch);
+  d.sp_rsun = rsun * L;
+  d.sp_rs = m.spiral.r_scale * L;
+  d.sp_hs = m.spiral.h_scale * L;
+  d.teu_n0 = m.te_unif.n0;
+  d.teu_r0 = m.te_unif.r0 * L;
+  d.tex_n0 = m.te_exp.n0;
+  d.tex_rs = m.te_exp.r_scale * L;
+  d.tex_hs = m.te_exp.h_scale * L;
+  if (m.cre == HXG_CRE_ANA) {
+    d.cre_alpha = m.cre_ana.alpha;
+    d.cre_beta = m.cre_ana.beta;
+    d.cre_theta = m.cre_ana.theta;
+    d.cre_r0 = m.cre_ana.r0 * L;
+    d.cre_z0 = m.cre_ana.z0 * L;
+  } else if (m.cre == HXG_CRE_UNIF) {
+    d.cre_alpha = m.cre_unif.alpha;
+    d.cre_unif_r0 = m.cre_unif.r0 * L;
+  }
+  d.cre_R0 = rsun * L;
+  return d;
+}
+
+int choose_chunks(const hxg_handle *h, uint64_t npix, uint64_t step) {
+  const double target = h->waves * h->sm_count * 2048.0;
+  int c = 1;
+  while (c < 32 && (double)npix * c < target && step / (2ull * c) >= 16) c *= 2;
+  return c;
+}
+
+// All launch constants of one shell (integrator.cc:136-228 semantics).
+int build_launch(hxg_handle *h, const hxg_obs_t &o, uint32_t s,
+                 ShellLaunch &P, uint64_t &step_out) {
+  const bool fp32 = h->precision == HXG_FP32C;
+  const double L = fp32 ? 1.0 / cgs::kpc : 1.0;
+  const double Bu = fp32 ? 1.0 / cgs::muGauss : 1.0;
+  const hxg_models_t &m = h->models;
+  std::memset(&P, 0, sizeof(P));
+  double d_start, delta;
+  uint64_t step;
+  shell_ref(o, s, d_start, delta, step);
+  step_out = step;
+  for (int i = 0; i < 3; ++i) P.obs[i] = o.observer[i] * L;
+  P.d_start = d_start * L;
+  P.delta = delta * L;
+  P.step = (long long)step;
+  P.gc_r_min = o.gc_r_min * L;
+  P.gc_r_max = o.gc_r_max * L;
+  P.gc_z_min = o.gc_z_min * L;
+  P.gc_z_max = o.gc_z_max * L;
+  P.nside = (int)o.nside_shell[s];
+  P.do_dm = o.do_dm != 0;
+  P.do_fd = o.do_fd != 0;
+  P.do_sync = o.do_sync != 0;
+  const double qe = cgs::qe, mec2 = cgs::mec2, c_l = cgs::c_light;
+  const double fdfore = -(qe * qe * qe) / (2. * cgs::pi * mec2 * mec2);
+  const double freq = o.sync_freq;
+  if (P.do_sync) {
+    P.lambda2 = (c_l / freq) * (c_l / freq);
+    P.i2bt = c_l * c_l / (2. * cgs::kB * freq * freq);
+    const double p = cgs::h_planck * freq / (cgs::kB * 2.725);
+    P.tc_a = std::exp(p) - 1.;
+    P.tc_b = p * p * std::exp(p);
+  } else {
+    P.tc_a = 1.;
+    P.tc_b = 1.;
+  }
+  P.models = dev_models(m, o.observer, L, Bu);
+  // analytic synchrotron emissivity constants (integrator.cc:332-346, 401-415)
+  if (P.do_sync) {
+    const double E0 = m.cre == HXG_CRE_ANA ? m.cre_ana.E0 : m.cre_unif.E0;
+    const double j0 = m.cre == HXG_CRE_ANA ? m.cre_ana.j0 : m.cre_unif.j0;
+    const double gamma0 = E0 / cgs::mec2;
+    const double beta0 = std::sqrt(1. - 1. / gamma0);
+    const double unit = 4. * cgs::pi * cgs::mec /
+                        (cgs::GeV * cgs::m * cgs::m * cgs::sec * beta0);
+    const double norm = j0 * std::pow(gamma0, -cre_index_at(m, o.observer));
+    P.em_n0u = norm * unit;
+    P.em_qe3 = qe * qe * qe;
+    P.em_anum = 2. * cgs::pi * freq * cgs::mec;
+    P.em_3qe = 3. * qe;
+    P.em_den_p = 16. * cgs::pi * mec2;
+    P.em_const = P.models.cre_const_index;
+    const double a_s = P.em_anum / (P.em_3qe * cgs::muGauss);
+    P.a_s = a_s;
+    const double kbase = P.em_n0u * 1.73205081 * P.em_qe3 * cgs::muGauss;
+    if (P.em_const) {
+      const double idx =
+          m.cre == HXG_CRE_ANA ? -m.cre_ana.alpha : -(m.cre_unif.alpha);
+      P.em_index = idx;
+      P.em_gt = std::tgamma(-0.25 * idx + 19. / 12.) * std::tgamma(-0.25 * idx - 1. / 12.);
+      P.em_gp = std::tgamma(-0.25 * idx + 7. / 12.) * std::tgamma(-0.25 * idx - 1. / 12.);
+      P.em_den_t = 4. * cgs::pi * mec2 * (1. - idx);
+      const double e = 0.5 * (idx + 1);
+      P.em_pow_kind = (e == -1.) ? 1 : (e == 0. ? 2 : 0);
+      P.em_pe = 1. - e;
+      const double ae = std::pow(a_s, e);
+      P.k_t = kbase / P.em_den_t * ae * P.em_gt * delta * P.i2bt;
+      P.k_p = kbase / P.em_den_p * ae * P.em_gp * delta * P.i2bt;
+    } else {
+      P.k_t = kbase / (4. * cgs::pi * mec2) * delta * P.i2bt;
+      P.k_p = kbase / P.em_den_p * delta * P.i2bt;
+    }
+  }
+  if (fp32) {
+    P.fd_fore = fdfore * delta * cgs::muGauss;
+    P.k_dm = delta;
+    P.phase_k = 2. * P.lambda2 * P.fd_fore;
+  } else {
+    P.fd_fore = fdfore;
+  }
+  // grid groups
+  P.ngroups = (int)h->groups.size();
+  for (size_t g = 0; g < h->groups.size(); ++g) {
+    const Group &G = h->groups[g];
+    DevGridGroup &D = P.groups[g];
+    D.rec = G.rec;
+    D.nx = (int)G.desc.nx;
+    D.ny = (int)G.desc.ny;
+    D.nz = (int)G.desc.nz;
+    D.has_b = G.b_slots[0] >= 0;
+    D.lo[0] = G.desc.x_min * L;
+    D.lo[1] = G.desc.y_min * L;
+    D.lo[2] = G.desc.z_min * L;
+    D.scale[0] = (double)(G.desc.nx - 1) / ((G.desc.x_max - G.desc.x_min) * L);
+    D.scale[1] = (double)(G.desc.ny - 1) / ((G.desc.y_max - G.desc.y_min) * L);
+    D.scale[2] = (double)(G.desc.nz - 1) / ((G.desc.z_max - G.desc.z_min) * L);
+  }
+  return HXG_OK;
+}
+
+int validate_obs(hxg_handle *h, const hxg_obs_t *o) {
+  if (!o) return fail(h, HXG_ERR_INVALID, "obs is NULL");
+  if (o->total_shell < 1 || o->total_shell > HXG_MAX_SHELLS)
+    return fail(h, HXG_ERR_INVALID, "total_shell %u out of [1,%d]", o->total_shell,
+                HXG_MAX_SHELLS);
+  for (uint32_t s = 0; s < o->total_shell; ++s) {
+    if (!is_pow2(o->nside_shell[s]) || o->nside_shell[s] > 8192)
+      return fail(h, HXG_ERR_INVALID, "nside_shell[%u]=%u is not a power of two <= 8192",
+                  s, o->nside_shell[s]);
+    if (!(o->radii_shell[s + 1] > o->radii_shell[s]))
+      return fail(h, HXG_ERR_INVALID, "shell %u has non-increasing radii", s);
+    double ds, dd;
+    uint64_t st;
+    shell_ref(*o, s, ds, dd, st);
+    if (st < 1 || st > (1ull << 40))
+      return fail(h, HXG_ERR_INVALID, "shell %u has %llu radial steps", s,
+                  (unsigned long long)st);
+  }
+  if (!(o->oc_r_res > 0.)) return fail(h, HXG_ERR_INVALID, "oc_r_res must be > 0");
+  if (o->do_dm && (!is_pow2(o->nside_dm) || o->nside_dm > 8192))
+    return fail(h, HXG_ERR_INVALID, "bad nside_dm %u", o->nside_dm);
+  if (o->do_fd && (!is_pow2(o->nside_fd) || o->nside_fd > 8192))
+    return fail(h, HXG_ERR_INVALID, "bad nside_fd %u", o->nside_fd);
+  if (o->do_sync) {
+    if (!is_pow2(o->nside_sync) || o->nside_sync > 8192)
+      return fail(h, HXG_ERR_INVALID, "bad nside_sync %u", o->nside_sync);
+    if (!(o->sync_freq > 0.)) return fail(h, HXG_ERR_INVALID, "sync_freq must be > 0");
+  }
+  if (o->do_mask && !h->have_mask)
+    return fail(h, HXG_ERR_STATE, "do_mask set but no mask uploaded");
+  return HXG_OK;
+}
+
+int upload_common(hxg_handle *h, int field, const hxg_grid_desc_t *g,
+                  const double *c0, const double *c1, const double *c2,
+                  cudaMemcpyKind kind) {
+  if (!h) return HXG_ERR_INVALID;
+  if (field < 0 || field > HXG_FIELD_CRE || !g)
+    return fail(h, HXG_ERR_INVALID, "bad field slot %d", field);
+  if (field == HXG_FIELD_CRE)
+    return fail(h, HXG_ERR_UNSUPPORTED, "CRE grids are not supported on the device");
+  if (g->nx < 2 || g->ny < 2 || g->nz < 2)
+    return fail(h, HXG_ERR_INVALID, "grid needs at least 2 vertices per axis");
+  if (!(g->x_max > g->x_min) || !(g->y_max > g->y_min) || !(g->z_max > g->z_min))
+    return fail(h, HXG_ERR_INVALID, "grid box has non-positive extent");
+  const bool vec = field == HXG_FIELD_BREG || field == HXG_FIELD_BRND;
+  const double *src[3] = {c0, c1, c2};
+  for (int k = 0; k < (vec ? 3 : 1); ++k)
+    if (!src[k]) return fail(h, HXG_ERR_INVALID, "grid component %d is NULL", k);
+  Slot &S = h->slots[field];
+  const size_t n = (size_t)g->nx * g->ny * g->nz;
+  if (S.present && S.n != n) {
+    for (auto &p : S.d)
+      if (p) cudaFree(p);
+    S.d[0] = S.d[1] = S.d[2] = nullptr;
+  }
+  for (int k = 0; k < (vec ? 3 : 1); ++k) {
+    if (!S.d[k]) {
+      cudaError_t e = cudaMalloc(&S.d[k], n * sizeof(double));
+      if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc(grid)");
+    }
+    HXG_CK(cudaMemcpyAsync(S.d[k], src[k], n * sizeof(double), kind, h->stream));
+  }
+  S.present = true;
+  S.n = n;
+  S.desc = *g;
+  h->groups_dirty = true;
+  return HXG_OK;
+}
+
+}  // namespace
+
+// ============================================================ C ABI ======
+extern "C" {
+
+int hxg_abi_version(void) { return HXG_ABI_VERSION; }
+
+int hxg_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+int hxg_create(int device, int precision, hxg_handle **out) {
+  if (!out) return HXG_ERR_INVALID;
+  *out = nullptr;
+  if (precision != HXG_FP64 && precision != HXG_FP32C) return HXG_ERR_INVALID;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return HXG_ERR_NO_DEVICE;
+  if (device < 0 || device >= n) return HXG_ERR_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return HXG_ERR_CUDA;
+  hxg_handle *h = new hxg_handle();
+  h->device = device;
+  h->precision = precision;
+  cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return HXG_ERR_CUDA;
+  }
+  h->stream = h->own_stream;
+  *out = h;
+  return HXG_OK;
+}
+
+int hxg_destroy(hxg_handle *h) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  free_groups(h);
+  clear_masks(h);
+  for (auto &s : h->slots)
+    for (auto &p : s.d)
+      if (p) cudaFree(p);
+  for (auto &b : h->tmp)
+    if (b.p) cudaFree(b.p);
+  for (auto &b : h->out)
+    if (b.p) cudaFree(b.p);
+  for (auto &e : h->events) {
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return HXG_OK;
+}
+
+const char *hxg_last_error(const hxg_handle *h) {
+  return h ? h->err.c_str() : "null handle";
+}
+
+int hxg_set_stream(hxg_handle *h, void *stream) {
+  if (!h) return HXG_ERR_INVALID;
+  h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+  return HXG_OK;
+}
+
+int hxg_set_models(hxg_handle *h, const hxg_models_t *m) {
+  if (!h || !m) return HXG_ERR_INVALID;
+  std::string why;
+  if (!models_supported(*m, &why)) return fail(h, HXG_ERR_UNSUPPORTED, "%s", why.c_str());
+  bool a0[4], a1[4];
+  active_slots(h->models, a0);
+  active_slots(*m, a1);
+  if (!h->have_models || std::memcmp(a0, a1, sizeof(a0)) != 0) h->groups_dirty = true;
+  h->models = *m;
+  h->have_models = true;
+  return HXG_OK;
+}
+
+int hxg_upload_grid(hxg_handle *h, int field, const hxg_grid_desc_t *g,
+                    const double *c0, const double *c1, const double *c2) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  const int st = upload_common(h, field, g, c0, c1, c2, cudaMemcpyHostToDevice);
+  if (st != HXG_OK) return st;
+  HXG_CK(cudaStreamSynchronize(h->stream));
+  return HXG_OK;
+}
+
+int hxg_upload_grid_device(hxg_handle *h, int field, const hxg_grid_desc_t *g,
+                           const double *d_c0, const double *d_c1,
+                           const double *d_c2) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  return upload_common(h, field, g, d_c0, d_c1, d_c2, cudaMemcpyDeviceToDevice);
+}
+
+int hxg_set_mask(hxg_handle *h, uint32_t nside, const double *mask) {
+  if (!h) return HXG_ERR_INVALID;
+  clear_masks(h);
+  if (!mask) {
+    h->have_mask = false;
+    h->mask_host.clear();
+    return HXG_OK;
+  }
+  if (!is_pow2(nside) || nside > 8192) return fail(h, HXG_ERR_INVALID, "bad mask nside %u", nside);
+  h->mask_host.assign(mask, mask + npix_of(nside));
+  h->mask_nside = nside;
+  h->have_mask = true;
+  return HXG_OK;
+}
+
+int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
+                          double *d_fd, double *d_is, double *d_qs,
+                          double *d_us) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  int st = validate_obs(h, o);
+  if (st != HXG_OK) return st;
+  if (!h->have_models) return fail(h, HXG_ERR_STATE, "models not set");
+  if (o->do_sync && h->models.cre == HXG_CRE_NONE)
+    return fail(h, HXG_ERR_INVALID, "synchrotron output needs a CRE model");
+  if ((o->do_dm && !d_dm) || (o->do_fd && !d_fd) ||
+      (o->do_sync && (!d_is || !d_qs || !d_us)))
+    return fail(h, HXG_ERR_INVALID, "an output requested by obs is NULL");
+  if ((st = build_groups(h)) != HXG_OK) return st;
+  const bool fp32 = h->precision == HXG_FP32C;
+  uint32_t max_nside = 0;
+  for (uint32_t s = 0; s < o->total_shell; ++s)
+    max_nside = std::max(max_nside, o->nside_shell[s]);
+  const size_t tbytes = npix_of(max_nside) * sizeof(double);
+  for (int k = 0; k < 5; ++k)
+    if ((st = ensure(h, h->tmp[k], tbytes)) != HXG_OK) return st;
+  double *tmp[5];
+  for (int k = 0; k < 5; ++k) tmp[k] = static_cast<double *>(h->tmp[k].p);
+  // Grid_obs maps start at zero (Grid_obs::build_grid, grid_obs.cc:21-43)
+  if (o->do_dm) HXG_CK(cudaMemsetAsync(d_dm, 0, npix_of(o->nside_dm) * 8, h->stream));
+  if (o->do_fd) HXG_CK(cudaMemsetAsync(d_fd, 0, npix_of(o->nside_fd) * 8, h->stream));
+  if (o->do_sync) {
+    const size_t b = npix_of(o->nside_sync) * 8;
+    HXG_CK(cudaMemsetAsync(d_is, 0, b, h->stream));
+    HXG_CK(cudaMemsetAsync(d_qs, 0, b, h->stream));
+    HXG_CK(cudaMemsetAsync(d_us, 0, b, h->stream));
+  }
+  for (uint32_t s = 0; s < o->total_shell; ++s) {
+    ShellLaunch P;
+    uint64_t step;
+    if ((st = build_launch(h, *o, s, P, step)) != HXG_OK) return st;
+    // inner-shell Faraday depth: the accumulated FD output map when it is
+    // requested, otherwise an all-zero map (integrator.cc:78-86, 130-132)
+    P.fdmap = o->do_fd ? d_fd : nullptr;
+    P.nside_fdmap = o->do_fd ? (int)o->nside_fd : 0;
+    P.mask = nullptr;
+    if (o->do_mask) {
+      const unsigned char *dm = nullptr;
+      if ((st = device_mask(h, o->nside_shell[s], &dm)) != HXG_OK) return st;
+      P.mask = dm;
+    }
+    for (int k = 0; k < 5; ++k) P.out[k] = tmp[k];
+    const uint64_t npix = npix_of(o->nside_shell[s]);
+    const int C = choose_chunks(h, npix, step);
+    P.chunks = C;
+    P.log2_chunks = hpx_ilog2((uint64_t)C);
+    const uint64_t warps = (npix + (32 / C) - 1) / (32 / C);
+    const unsigned threads = 256;
+    const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (h->timing) {
+      HXG_CK(cudaEventCreate(&e0));
+      HXG_CK(cudaEventCreate(&e1));
+      HXG_CK(cudaEventRecord(e0, h->stream));
+    }
+    HXG_CK(launch_shell(h->stream, fp32, P, blocks, threads));
+    ++h->launch_count;
+    if (h->timing) {
+      HXG_CK(cudaEventRecord(e1, h->stream));
+      h->events.emplace_back(e0, e1);
+      h->event_samples.push_back((int64_t)(npix * step));
+    }
+    // accumulate the shell maps into the outputs (integrator.cc:121-132)
+    const int ns = (int)o->nside_shell[s];
+    if (o->do_dm) {
+      double *d[1] = {d_dm};
+      const double *sr[1] = {tmp[0]};
+      HXG_CK(launch_accumulate(h->stream, (int)o->nside_dm, ns, 1, d, sr));
+      ++h->launch_count;
+    }
+    if (o->do_sync) {
+      double *d[3] = {d_is, d_qs, d_us};
+      const double *sr[3] = {tmp[2], tmp[3], tmp[4]};
+      HXG_CK(launch_accumulate(h->stream, (int)o->nside_sync, ns, 3, d, sr));
+      ++h->launch_count;
+    }
+    if (o->do_fd) {
+      double *d[1] = {d_fd};
+      const double *sr[1] = {tmp[1]};
+      HXG_CK(launch_accumulate(h->stream, (int)o->nside_fd, ns, 1, d, sr));
+      ++h->launch_count;
+    }
+  }
+  return HXG_OK;
+}
+
+int hxg_write_grid(hxg_handle *h, const hxg_obs_t *o, double *dm, double *fd,
+                   double *is, double *qs, double *us) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  int st = validate_obs(h, o);
+  if (st != HXG_OK) return st;
+  if ((o->do_dm && !dm) || (o->do_fd && !fd) || (o->do_sync && (!is || !qs || !us)))
+    return fail(h, HXG_ERR_INVALID, "an output requested by obs is NULL");
+  const size_t b_dm = o->do_dm ? npix_of(o->nside_dm) * 8 : 8;
+  const size_t b_fd = o->do_fd ? npix_of(o->nside_fd) * 8 : 8;
+  const size_t b_sy = o->do_sync ? npix_of(o->nside_sync) * 8 : 8;
+  const size_t bytes[5] = {b_dm, b_fd, b_sy, b_sy, b_sy};
+  for (int k = 0; k < 5; ++k)
+    if ((st = ensure(h, h->out[k], bytes[k])) != HXG_OK) return st;
+  double *d[5];
+  for (int k = 0; k < 5; ++k) d[k] = static_cast<double *>(h->out[k].p);
+  st = hxg_write_grid_device(h, o, d[0], d[1], d[2], d[3], d[4]);
+  if (st != HXG_OK) return st;
+  double *host[5] = {dm, fd, is, qs, us};
+  const bool want[5] = {o->do_dm != 0, o->do_fd != 0, o->do_sync != 0,
+                        o->do_sync != 0, o->do_sync != 0};
+  for (int k = 0; k < 5; ++k)
+    if (want[k])
+      HXG_CK(cudaMemcpyAsync(host[k], d[k], bytes[k], cudaMemcpyDeviceToHost, h->stream));
+  HXG_CK(cudaStreamSynchronize(h->stream));
+  return HXG_OK;
+}
+
+int hxg_sync(hxg_handle *h) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  HXG_CK(cudaStreamSynchronize(h->stream));
+  HXG_CK(cudaGetLastError());
+  return HXG_OK;
+}
+
+int hxg_set_timing(hxg_handle *h, int enable) {
+  if (!h) return HXG_ERR_INVALID;
+  h->timing = enable != 0;
+  h->acc_ms = 0.;
+  h->acc_launches = h->acc_samples = 0;
+  for (auto &e : h->events) {
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
+  h->events.clear();
+  h->event_samples.clear();
+  return HXG_OK;
+}
+
+int hxg_get_timing(hxg_handle *h, double *kernel_ms, int64_t *launches,
+                   int64_t *samples) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  HXG_CK(cudaStreamSynchronize(h->stream));
+  for (size_t i = 0; i < h->events.size(); ++i) {
+    float ms = 0.f;
+    HXG_CK(cudaEventElapsedTime(&ms, h->events[i].first, h->events[i].second));
+    h->acc_ms += ms;
+    h->acc_launches += 1;
+    h->acc_samples += h->event_samples[i];
+    cudaEventDestroy(h->events[i].first);
+    cudaEventDestroy(h->events[i].second);
+  }
+  h->events.clear();
+  h->event_samples.clear();
+  if (kernel_ms) *kernel_ms = h->acc_ms;
+  if (launches) *launches = h->acc_launches;
+  if (samples) *samples = h->acc_samples;
+  return HXG_OK;
+}
+
+int hxg_get_launch_count(hxg_handle *h, int64_t *count) {
+  if (!h || !count) return HXG_ERR_INVALID;
+  *count = h->launch_count;
+  return HXG_OK;
+}
+
+int hxg_shell_ref(const hxg_obs_t *obs, uint32_t shell, double *d_start,
+                  double *delta_d, uint64_t *step) {
+  if (!obs || !d_start || !delta_d || !step || shell >= obs->total_shell ||
+      obs->total_shell > HXG_MAX_SHELLS)
+    return HXG_ERR_INVALID;
+  shell_ref(*obs, shell, *d_start, *delta_d, *step);
+  return HXG_OK;
+}
+
+int hxg_mask_duplicate(uint32_t pivot_nside, const double *pivot_mask,
+                       uint32_t nside, double *out) {
+  if (!pivot_mask || !out || !is_pow2(pivot_nside) || !is_pow2(nside) ||
+      pivot_nside > 8192 || nside > 8192)
+    return HXG_ERR_INVALID;
+  mask_duplicate_host(pivot_nside, pivot_mask, nside, out);
+  return HXG_OK;
+}
+
+// ---- device known-answer helpers ----------------------------------------
+namespace {
+struct Scratch {
+  std::vector<void *> ptrs;
+  ~Scratch() {
+    for (void *p : ptrs) cudaFree(p);
+  }
+  double *alloc(size_t n) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, n * sizeof(double) + 8) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return static_cast<double *>(p);
+  }
+};
+
+int kat_status(cudaError_t e) {
+  if (e == cudaSuccess) return HXG_OK;
+  return e == cudaErrorMemoryAllocation ? HXG_ERR_OOM : HXG_ERR_CUDA;
+}
+
+#define KAT_ALLOC(var, n) \
+  double *var = S.alloc(n); \
+  if (!var) return HXG_ERR_OOM;
+#define KAT_CK(call)                          \
+  do {                                        \
+    const int s_ = kat_status(call);          \
+    if (s_ != HXG_OK) return s_;              \
+  } while (0)
+
+int kat_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return HXG_ERR_NO_DEVICE;
+  return HXG_OK;
+}
+}  // namespace
+
+int hxg_pix2ang(uint32_t nside, uint64_t npix, double *theta, double *phi) {
+  if (!theta || !phi || !is_pow2(nside) || nside > 8192 || npix > npix_of(nside))
+    return HXG_ERR_INVALID;
+  if (kat_device() != HXG_OK) return HXG_ERR_NO_DEVICE;
+  Scratch S;
+  KAT_ALLOC(dt, npix);
+  KAT_ALLOC(dp, npix);
+  KAT_CK(launch_pix2ang(0, (int)nside, npix, dt, dp));
+  KAT_CK(cudaMemcpy(theta, dt, npix * 8, cudaMemcpyDeviceToHost));
+  KAT_CK(cudaMemcpy(phi, dp, npix * 8, cudaMemcpyDeviceToHost));
+  return HXG_OK;
+}
+
+int hxg_interpolate(uint32_t nside, const double *map, uint64_t n,
+                    const double *theta, const double *phi, double *out) {
+  if (!map || !theta || !phi || !out || !is_pow2(nside) || nside > 8192)
+    return HXG_ERR_INVALID;
+  if (kat_device() != HXG_OK) return HXG_ERR_NO_DEVICE;
+  Scratch S;
+  const uint64_t np = npix_of(nside);
+  KAT_ALLOC(dm, np);
+  KAT_ALLOC(dt, n);
+  KAT_ALLOC(dp, n);
+  KAT_ALLOC(dout, n);
+  KAT_CK(cudaMemcpy(dm, map, np * 8, cudaMemcpyHostToDevice));
+  KAT_CK(cudaMemcpy(dt, theta, n * 8, cudaMemcpyHostToDevice));
+  KAT_CK(cudaMemcpy(dp, phi, n * 8, cudaMemcpyHostToDevice));
+  KAT_CK(launch_interpolate(0, (int)nside, dm, n, dt, dp, dout));
+  KAT_CK(cudaMemcpy(out, dout, n * 8, cudaMemcpyDeviceToHost));
+  return HXG_OK;
+}
+
+int hxg_accumulate(uint32_t nside_dst, double *dst, uint32_t nside_src,
+                   const double *src) {
+  if (!dst || !src || !is_pow2(nside_dst) || !is_pow2(nside_src) ||
+      nside_dst > 8192 || nside_src > 8192)
+    return HXG_ERR_INVALID;
+  if (kat_device() != HXG_OK) return HXG_ERR_NO_DEVICE;
+  Scratch S;
+  const uint64_t nd = npix_of(nside_dst), ns = npix_of(nside_src);
+  KAT_ALLOC(dd, nd);
+  KAT_ALLOC(ds, ns);
+  KAT_CK(cudaMemcpy(dd, dst, nd * 8, cudaMemcpyHostToDevice));
+  KAT_CK(cudaMemcpy(ds, src, ns * 8, cudaMemcpyHostToDevice));
+  double *d[1] = {dd};
+  const double *s[1] = {ds};
+  KAT_CK(launch_accumulate(0, (int)nside_dst, (int)nside_src, 1, d, s));
+  KAT_CK(cudaMemcpy(dst, dd, nd * 8, cudaMemcpyDeviceToHost));
+  return HXG_OK;
+}
+
+int hxg_los_geometry(uint64_t n, const double *theta, const double *phi,
+                     const double *b, double *versor, double *b_par,
+                     double *b_per, double *cos2ipa, double *sin2ipa) {
+  if (!theta || !phi || !b || !versor || !b_par || !b_per || !cos2ipa || !sin2ipa)
+    return HXG_ERR_INVALID;
+  if (kat_device() != HXG_OK) return HXG_ERR_NO_DEVICE;
+  Scratch S;
+  KAT_ALLOC(dt, n);
+  KAT_ALLOC(dp, n);
+  KAT_ALLOC(db, 3 * n);
+  KAT_ALLOC(dv, 3 * n);
+  KAT_ALLOC(dpar, n);
+  KAT_ALLOC(dper, n);
+  KAT_ALLOC(dc, n);
+  KAT_ALLOC(ds, n);
+  KAT_CK(cudaMemcpy(dt, theta, n * 8, cudaMemcpyHostToDevice));
+  KAT_CK(cudaMemcpy(dp, phi, n * 8, cudaMemcpyHostToDevice));
+  KAT_CK(cudaMemcpy(db, b, 3 * n * 8, cudaMemcpyHostToDevice));
+  KAT_CK(launch_los_geometry(0, n, dt, dp, db, dv, dpar, dper, dc, ds));
+  KAT_CK(cudaMemcpy(versor, dv, 3 * n * 8, cudaMemcpyDeviceToHost));
+  KAT_CK(cudaMemcpy(b_par, dpar, n * 8, cudaMemcpyDeviceToHost));
+  KAT_CK(cudaMemcpy(b_per, dper, n * 8, cudaMemcpyDeviceToHost));
+  KAT_CK(cudaMemcpy(cos2ipa, dc, n * 8, cudaMemcpyDeviceToHost));
+  KAT_CK(cudaMemcpy(sin2ipa, ds, n * 8, cudaMemcpyDeviceToHost));
+  return HXG_OK;
+}
+
+int hxg_read_grid(hxg_handle *h, int field, uint64_t n, const double *pos,
+                  double *out) {
+  if (!h || !pos || !out || field < 0 || field > HXG_FIELD_TERND)
+    return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  if (!h->have_models) return fail(h, HXG_ERR_STATE, "models not set");
+  int st = build_groups(h);
+  if (st != HXG_OK) return st;
+  const Group *G = nullptr;
+  for (const auto &g : h->groups)
+    for (int k = 0; k < 2; ++k)
+      if (g.b_slots[k] == field || g.t_slots[k] == field) G = &g;
+  if (!G) return fail(h, HXG_ERR_STATE, "grid slot %d is not read by the models", field);
+  const bool fp32 = h->precision == HXG_FP32C;
+  const double L = fp32 ? 1.0 / cgs::kpc : 1.0;
+  DevGridGroup D{};
+  D.rec = G->rec;
+  D.nx = (int)G->desc.nx;
+  D.ny = (int)G->desc.ny;
+  D.nz = (int)G->desc.nz;
+  D.lo[0] = G->desc.x_min * L;
+  D.lo[1] = G->desc.y_min * L;
+  D.lo[2] = G->desc.z_min * L;
+  D.scale[0] = (double)(G->desc.nx - 1) / ((G->desc.x_max - G->desc.x_min) * L);
+  D.scale[1] = (double)(G->desc.ny - 1) / ((G->desc.y_max - G->desc.y_min) * L);
+  D.scale[2] = (double)(G->desc.nz - 1) / ((G->desc.z_max - G->desc.z_min) * L);
+  std::vector<double> p(3 * n), res(4 * n);
+  for (uint64_t i = 0; i < 3 * n; ++i) p[i] = pos[i] * L;
+  Scratch S;
+  double *dpos = S.alloc(3 * n), *dout = S.alloc(4 * n);
+  if (!dpos || !dout) return fail(h, HXG_ERR_OOM, "scratch");
+  HXG_CK(cudaMemcpy(dpos, p.data(), 3 * n * 8, cudaMemcpyHostToDevice));
+  HXG_CK(launch_read_group(0, fp32, D, n, dpos, dout));
+  HXG_CK(cudaMemcpy(res.data(), dout, 4 * n * 8, cudaMemcpyDeviceToHost));
+  const double bu = fp32 ? cgs::muGauss : 1.0;
+  const bool vec = field == HXG_FIELD_BREG || field == HXG_FIELD_BRND;
+  for (uint64_t i = 0; i < n; ++i) {
+    if (vec)
+      for (int k = 0; k < 3; ++k) out[3 * i + k] = res[4 * i + k] * bu;
+    else
+      out[i] = res[4 * i + 3];
+  }
+  return HXG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,391 @@
+// hxg_integrate.cuh -- shell integration kernels (the per-pixel radial loop
+// of Integrator::radial_integration, source/integrator/integrator.cc:136-228,
+// run for every pixel of one shell, integrator.cc:60-116).
+//
+// Mapping: each warp owns 32/C pixels of a compact NESTED sky patch (so
+// neighbouring rays share grid cache lines) and C lanes split each pixel's
+// radial range into contiguous chunks.  Chunk c integrates with the phase of
+// its own partial Faraday depth; once the chunk sums are known, its Stokes
+// Q/U are rotated by 2*lambda^2*(Faraday depth of the chunks before it) --
+// algebraically identical to the reference's running phase
+// (integrator.cc:221-225) -- and the chunks are reduced with warp shuffles.
+// With C = 1 (large shells) each lane is one pixel in the reference's order.
+#pragma once
+
+#include "hxg_common.cuh"
+#include "hxg_fields.cuh"
+
+namespace hxg {
+
+constexpr int kMaxGroups = 4;
+
+// Everything one shell launch needs, in the working units of its form.
+struct ShellLaunch {
+  double obs[3];             // observer
+  double d_start, delta;     // first-sample distance and radial step
+  long long step;            // samples per ray (integrator.cc:237-240)
+  double gc_r_min, gc_r_max, gc_z_min, gc_z_max;
+  int nside, chunks, log2_chunks;
+  int do_dm, do_fd, do_sync;
+  const double *fdmap;       // accumulated FD map of inner shells (or null)
+  int nside_fdmap;
+  const unsigned char *mask; // 1 = integrate (integrator.cc:69-70), or null
+  double *out[5];            // shell maps (RING): dm, fd, is, qs, us
+  // FD and synchrotron constants
+  double fd_fore;            // FP64: -qe^3/(2 pi mec2^2); FP32C: that * delta * muG
+  double lambda2;            // (c/nu)^2
+  double i2bt;               // c^2 / (2 kB nu^2)
+  double tc_a, tc_b;         // temp_convert(t) = t*a*a/b (integrator.cc:275-279)
+  // analytic synchrotron emissivity (integrator.cc:332-346, 401-415)
+  int em_const;              // spectral index constant over space
+  int em_pow_kind;           // 0: pow(); 1: exponent == -1; 2: exponent == 0
+  double em_index;           // constant index
+  double em_n0u;             // j0 * gamma0^-index(observer) * unit
+  double em_qe3, em_den_t, em_den_p, em_anum, em_3qe;
+  double em_gt, em_gp;       // Gamma products at the constant index
+  // FP32C scales (applied in FP64 after the sums)
+  double k_t, k_p, k_dm;     // I, Q/U and DM scale factors
+  double phase_k;            // 2 lambda^2 * fd_fore (per FP64 FD-sum unit)
+  double a_s;                // A * |B_perp| in muG (variable-index path)
+  double em_pe;              // exponent of |B_perp| (constant index, FP32C)
+  DevModels models;
+  DevGridGroup groups[kMaxGroups];
+  int ngroups;
+};
+
+// Kahan-compensated FP32 accumulator.
+struct KahanF {
+  float s, c;
+  __device__ __forceinline__ void add(float v) {
+    const float y = v - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ __forceinline__ double value() const {
+    return double(s) - double(c);
+  }
+};
+
+__device__ __forceinline__ double shfl_xor_d(double v, int o) {
+  return __shfl_xor_sync(0xffffffffu, v, o);
+}
+
+// Combine the C chunk partial sums of each pixel: exclusive FD prefix over
+// the chunks, rotation of each chunk's Q/U by 2*lambda^2*prefix, butterfly
+// reduction inside the C-lane segment.  All 32 lanes participate.
+__device__ __forceinline__ void combine_chunks(const ShellLaunch &P, int c,
+                                               double rot_k, double &dm,
+                                               double &fd, double &si,
+                                               double &sq, double &su) {
+  const int C = P.chunks;
+  if (C == 1) return;
+  // inclusive scan of fd within the segment
+  double incl = fd;
+  for (int o = 1; o < C; o <<= 1) {
+    const double v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (c >= o) incl += v;
+  }
+  double excl = __shfl_up_sync(0xffffffffu, incl, 1);
+  if (c == 0) excl = 0.;
+  if (P.do_sync && c > 0) {
+    double sr, cr;
+    sincos(rot_k * excl, &sr, &cr);
+    const double q = sq * cr - su * sr;
+    const double u = sq * sr + su * cr;
+    sq = q;
+    su = u;
+  }
+  for (int o = C >> 1; o > 0; o >>= 1) {
+    dm += shfl_xor_d(dm, o);
+    fd += shfl_xor_d(fd, o);
+    si += shfl_xor_d(si, o);
+    sq += shfl_xor_d(sq, o);
+    su += shfl_xor_d(su, o);
+  }
+}
+
+// cos(2*ipa), sin(2*ipa) of the IAU polarisation angle
+// ipa = atan2(-e_theta.B, -e_phi.B) (integrator.cc:257-265), from the
+// double-angle identities (no atan2).
+template <typename T>
+__device__ __forceinline__ void ipa2(T xv, T yv, T &c2, T &s2) {
+  const T r2 = xv * xv + yv * yv;
+  if (r2 > T(0)) {
+    const T inv = T(1) / r2;
+    c2 = (xv * xv - yv * yv) * inv;
+    s2 = T(2) * xv * yv * inv;
+  } else {
+    c2 = T(1);
+    s2 = T(0);
+  }
+}
+
+// ===================================================================
+// FP64 parity form
+// ===================================================================
+template <int NG, bool kCache>
+__global__ void __launch_bounds__(256)
+shell_fp64_kernel(const ShellLaunch P) {
+  const int lane = threadIdx.x & 31;
+  const long long gw =
+      ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int C = P.chunks;
+  const int seg = lane >> P.log2_chunks;
+  const int c = lane & (C - 1);
+  const Hpx h = hpx_make((uint64_t)P.nside);
+  const unsigned long long nest =
+      (unsigned long long)gw * (32 >> P.log2_chunks) + seg;
+  const bool valid = nest < h.npix;
+  uint64_t ring = 0;
+  bool live = false;
+  if (valid) {
+    ring = hpx_nest2ring(h, nest);
+    live = (P.mask == nullptr) || (P.mask[ring] != 0);
+  }
+  double dm = 0., fd = 0., si = 0., sq = 0., su = 0.;
+  const double rot_k = 2. * P.lambda2;
+  if (live) {
+    double th, ph;
+    hpx_pix2ang(h, ring, th, ph);
+    double inner = 0.;
+    if (P.fdmap != nullptr) {
+      const Hpx hf = hpx_make((uint64_t)P.nside_fdmap);
+      inner = hpx_interpolate(hf, P.fdmap, th, ph);
+    }
+    const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
+    // los_versor (integrator.cc:268-272)
+    const double ux = cp * st, uy = sp * st, uz = ct;
+    // spherical unit vectors of sync_ipa (integrator.cc:260-262)
+    const double etx = ct * cp, ety = ct * sp, etz = -st;
+    const double epx = -sp, epy = cp;
+    const DevModels &M = P.models;
+    CellCache<double> cache;
+    cache.key = -1;
+    double last_index = nan(""), gt = P.em_gt, gp = P.em_gp;
+    const long long i0 = (P.step * c) >> P.log2_chunks;
+    const long long i1 = (P.step * (c + 1)) >> P.log2_chunks;
+    for (long long i = i0; i < i1; ++i) {
+      const double d = P.d_start + ((double)i + 0.5) * P.delta;
+      const double px = ux * d + P.obs[0];
+      const double py = uy * d + P.obs[1];
+      const double pz = uz * d + P.obs[2];
+      const double len = sqrt(px * px + py * py + pz * pz);
+      if (len < P.gc_r_min || len > P.gc_r_max || pz < P.gc_z_min ||
+          pz > P.gc_z_max)
+        continue;
+      V3<double> B = breg_model<double>(M, px, py, pz);
+      double te = tereg_model<double>(M, px, py, pz);
+      if (NG > 0) {
+        double b3[3] = {B.x, B.y, B.z};
+#pragma unroll 1
+        for (int g = 0; g < (NG == 1 ? 1 : P.ngroups); ++g)
+          sample_group<double, kCache>(P.groups[g], px, py, pz, cache, b3, te);
+        B.x = b3[0];
+        B.y = b3[1];
+        B.z = b3[2];
+      }
+      te *= (double)(te > 0.);
+      const double bpar = B.x * ux + B.y * uy + B.z * uz;
+      const double cx = B.y * uz - B.z * uy;
+      const double cy = B.z * ux - B.x * uz;
+      const double cz = B.x * uy - B.y * ux;
+      const double bper = sqrt(cx * cx + cy * cy + cz * cz);
+      if (P.do_dm) dm += te * P.delta;
+      if (P.do_fd || P.do_sync) fd += te * bpar * P.fd_fore * P.delta;
+      if (P.do_sync) {
+        double index = P.em_index;
+        if (!P.em_const) {
+          index = cre_index<double>(M, px, py, pz);
+          if (index != last_index) {
+            gt = tgamma(-0.25 * index + 19. / 12.) * tgamma(-0.25 * index - 1. / 12.);
+            gp = tgamma(-0.25 * index + 7. / 12.) * tgamma(-0.25 * index - 1. / 12.);
+            last_index = index;
+          }
+        }
+        const double fn = P.em_n0u * cre_profile<double>(M, px, py, pz);
+        const double absb = fabs(bper);
+        const double A = P.em_anum / (P.em_3qe * absb);
+        double Ae;
+        if (P.em_const && P.em_pow_kind == 1)
+          Ae = 1. / A;
+        else if (P.em_const && P.em_pow_kind == 2)
+          Ae = 1.;
+        else
+          Ae = pow(A, 0.5 * (index + 1));
+        const double den_t = P.em_const ? P.em_den_t
+                                        : 4. * cgs::pi * cgs::mec2 * (1. - index);
+        const double norm_t = fn * 1.73205081 * P.em_qe3 * absb / den_t;
+        const double norm_p = fn * 1.73205081 * P.em_qe3 * absb / P.em_den_p;
+        const double jtot = norm_t * (Ae * gt) * P.delta * P.i2bt;
+        const double jpol = norm_p * (Ae * gp) * P.delta * P.i2bt;
+        si += jtot;
+        double c2, s2;
+        ipa2<double>(-(epx * B.x + epy * B.y), -(etx * B.x + ety * B.y + etz * B.z),
+                     c2, s2);
+        double sf, cf;
+        sincos(2. * ((inner + fd) * P.lambda2), &sf, &cf);
+        sq += (cf * c2 - sf * s2) * jpol;
+        su += (sf * c2 + cf * s2) * jpol;
+      }
+    }
+  }
+  combine_chunks(P, c, rot_k, dm, fd, si, sq, su);
+  if (live && c == 0) {
+    if (P.do_dm) P.out[0][ring] = dm;
+    if (P.do_fd || P.do_sync) P.out[1][ring] = fd;
+    if (P.do_sync) {
+      P.out[2][ring] = si * P.tc_a * P.tc_a / P.tc_b;
+      P.out[3][ring] = sq * P.tc_a * P.tc_a / P.tc_b;
+      P.out[4][ring] = su * P.tc_a * P.tc_a / P.tc_b;
+    }
+  } else if (valid && !live && c == 0) {
+    // masked pixel: every observable is zero (integrator.cc:63-67, 98-115)
+    if (P.do_dm) P.out[0][ring] = 0.;
+    if (P.do_fd || P.do_sync) P.out[1][ring] = 0.;
+    if (P.do_sync) P.out[2][ring] = P.out[3][ring] = P.out[4][ring] = 0.;
+  }
+}
+
+// ===================================================================
+// FP32-compensated form
+// ===================================================================
+template <int NG, bool kCache>
+__global__ void __launch_bounds__(256)
+shell_fp32c_kernel(const ShellLaunch P) {
+  const int lane = threadIdx.x & 31;
+  const long long gw =
+      ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int C = P.chunks;
+  const int seg = lane >> P.log2_chunks;
+  const int c = lane & (C - 1);
+  const Hpx h = hpx_make((uint64_t)P.nside);
+  const unsigned long long nest =
+      (unsigned long long)gw * (32 >> P.log2_chunks) + seg;
+  const bool valid = nest < h.npix;
+  uint64_t ring = 0;
+  bool live = false;
+  if (valid) {
+    ring = hpx_nest2ring(h, nest);
+    live = (P.mask == nullptr) || (P.mask[ring] != 0);
+  }
+  double dm = 0., fd = 0., si = 0., sq = 0., su = 0.;
+  if (live) {
+    // FP64: pointing, LOS versor and inner-shell Faraday depth
+    double th, ph;
+    hpx_pix2ang(h, ring, th, ph);
+    double inner = 0.;
+    if (P.fdmap != nullptr) {
+      const Hpx hf = hpx_make((uint64_t)P.nside_fdmap);
+      inner = hpx_interpolate(hf, P.fdmap, th, ph);
+    }
+    const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
+    const double ux = cp * st, uy = sp * st, uz = ct;
+    const float uxf = float(ux), uyf = float(uy), uzf = float(uz);
+    const float etx = float(ct * cp), ety = float(ct * sp), etz = float(-st);
+    const float epx = float(-sp), epy = float(cp);
+    const double r2min = P.gc_r_min * P.gc_r_min, r2max = P.gc_r_max * P.gc_r_max;
+    const double phi0 = 2. * P.lambda2 * inner;
+    const DevModels &M = P.models;
+    const float pe = float(P.em_pe);
+    const float a_s = float(P.a_s);
+    CellCache<float> cache;
+    cache.key = -1;
+    KahanF kdm{0.f, 0.f}, ki{0.f, 0.f}, kq{0.f, 0.f}, ku{0.f, 0.f};
+    double sfd = 0.;
+    float last_index = __int_as_float(0x7fc00000), gt = float(P.em_gt),
+          gp = float(P.em_gp), inv1mi = 1.f;
+    const long long i0 = (P.step * c) >> P.log2_chunks;
+    const long long i1 = (P.step * (c + 1)) >> P.log2_chunks;
+    double dd = P.d_start + ((double)i0 + 0.5) * P.delta;
+    for (long long i = i0; i < i1; ++i, dd += P.delta) {
+      const double d = P.d_start + ((double)i + 0.5) * P.delta;
+      const double px = fma(ux, d, P.obs[0]);
+      const double py = fma(uy, d, P.obs[1]);
+      const double pz = fma(uz, d, P.obs[2]);
+      const double r2 = fma(px, px, fma(py, py, pz * pz));
+      if (r2 < r2min || r2 > r2max || pz < P.gc_z_min || pz > P.gc_z_max)
+        continue;
+      const float x = float(px), y = float(py), z = float(pz);
+      V3<float> B = breg_model<float>(M, x, y, z);
+      float te = tereg_model<float>(M, x, y, z);
+      if (NG > 0) {
+        float b3[3] = {B.x, B.y, B.z};
+#pragma unroll 1
+        for (int g = 0; g < (NG == 1 ? 1 : P.ngroups); ++g)
+          sample_group<float, kCache>(P.groups[g], px, py, pz, cache, b3, te);
+        B.x = b3[0];
+        B.y = b3[1];
+        B.z = b3[2];
+      }
+      te = te > 0.f ? te : 0.f;
+      const float bpar = B.x * uxf + B.y * uyf + B.z * uzf;
+      const float cx = B.y * uzf - B.z * uyf;
+      const float cy = B.z * uxf - B.x * uzf;
+      const float cz = B.x * uyf - B.y * uxf;
+      const float bper = sqrtf(cx * cx + cy * cy + cz * cz);
+      if (P.do_dm) kdm.add(te);
+      if (P.do_fd || P.do_sync) sfd += double(te * bpar);
+      if (P.do_sync) {
+        const float prof = cre_profile<float>(M, x, y, z);
+        float wt, wp;
+        if (P.em_const) {
+          float bp;
+          if (pe == 2.f)
+            bp = bper * bper;
+          else if (pe == 1.f)
+            bp = bper;
+          else
+            bp = powf(bper, pe);
+          wt = wp = prof * bp;
+        } else {
+          const float index = cre_index<float>(M, x, y, z);
+          if (index != last_index) {
+            gt = tgammaf(-0.25f * index + 19.f / 12.f) * tgammaf(-0.25f * index - 1.f / 12.f);
+            gp = tgammaf(-0.25f * index + 7.f / 12.f) * tgammaf(-0.25f * index - 1.f / 12.f);
+            inv1mi = 1.f / (1.f - index);
+            last_index = index;
+          }
+          const float Ae = exp2f(0.5f * (index + 1.f) * log2f(a_s / bper));
+          const float base = prof * bper * Ae;
+          wt = base * gt * inv1mi;
+          wp = base * gp;
+        }
+        ki.add(wt);
+        float c2, s2;
+        ipa2<float>(-(epx * B.x + epy * B.y), -(etx * B.x + ety * B.y + etz * B.z),
+                    c2, s2);
+        // FP64 Faraday phase, reduced to [-pi, pi] before FP32 sincos
+        const double phi = fma(P.phase_k, sfd, phi0);
+        const double kk = rint(phi * (1. / cgs::twopi));
+        const float rph = float(fma(-kk, cgs::twopi, phi));
+        float sf, cf;
+        sincosf(rph, &sf, &cf);
+        kq.add(wp * (cf * c2 - sf * s2));
+        ku.add(wp * (sf * c2 + cf * s2));
+      }
+    }
+    (void)dd;
+    dm = kdm.value() * P.k_dm;
+    fd = sfd * P.fd_fore;
+    si = ki.value() * P.k_t;
+    sq = kq.value() * P.k_p;
+    su = ku.value() * P.k_p;
+  }
+  combine_chunks(P, c, 2. * P.lambda2, dm, fd, si, sq, su);
+  if (live && c == 0) {
+    if (P.do_dm) P.out[0][ring] = dm;
+    if (P.do_fd || P.do_sync) P.out[1][ring] = fd;
+    if (P.do_sync) {
+      P.out[2][ring] = si * P.tc_a * P.tc_a / P.tc_b;
+      P.out[3][ring] = sq * P.tc_a * P.tc_a / P.tc_b;
+      P.out[4][ring] = su * P.tc_a * P.tc_a / P.tc_b;
+    }
+  } else if (valid && !live && c == 0) {
+    if (P.do_dm) P.out[0][ring] = 0.;
+    if (P.do_fd || P.do_sync) P.out[1][ring] = 0.;
+    if (P.do_sync) P.out[2][ring] = P.out[3][ring] = P.out[4][ring] = 0.;
+  }
+}
+
+}  // namespace hxg

@@ -1,0 +1,214 @@
+// hxg_kernels.cu -- map kernels (shell merge, HEALPix helpers), grid
+// packing, and the instantiations of the shell-integration kernels.
+#include <cuda_runtime.h>
+
+#include "hxg_integrate.cuh"
+#include "hxg_internal.h"
+
+namespace hxg {
+
+// ---- Hampix::accumulate (include/hamdis.h:698-721) ----------------------
+// dst_k += src_k for up to 3 map pairs sharing one (nside_dst, nside_src);
+// when the Nsides differ, src is interpolated at each dst pixel's pointing.
+__global__ void accumulate_kernel(int nside_dst, int nside_src, int nmaps,
+                                  double *d0, const double *s0, double *d1,
+                                  const double *s1, double *d2,
+                                  const double *s2) {
+  const Hpx hd = hpx_make((uint64_t)nside_dst);
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= hd.npix) return;
+  double *dst[3] = {d0, d1, d2};
+  const double *src[3] = {s0, s1, s2};
+  if (nside_dst == nside_src) {
+    for (int k = 0; k < nmaps; ++k) dst[k][i] = dst[k][i] + src[k][i];
+    return;
+  }
+  const Hpx hs = hpx_make((uint64_t)nside_src);
+  double th, ph;
+  hpx_pix2ang(hd, i, th, ph);
+  uint64_t pix[4];
+  double w[4];
+  hpx_interp_weights(hs, th, ph, pix, w);
+  for (int k = 0; k < nmaps; ++k)
+    dst[k][i] = dst[k][i] + hpx_interp_apply(src[k], pix, w);
+}
+
+__global__ void pix2ang_kernel(int nside, uint64_t n, double *theta,
+                               double *phi) {
+  const Hpx h = hpx_make((uint64_t)nside);
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || i >= h.npix) return;
+  hpx_pix2ang(h, i, theta[i], phi[i]);
+}
+
+__global__ void interpolate_kernel(int nside, const double *map, uint64_t n,
+                                   const double *theta, const double *phi,
+                                   double *out) {
+  const Hpx h = hpx_make((uint64_t)nside);
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double th = theta[i], ph = phi[i];
+  hamp_norm(th, ph);
+  out[i] = hpx_interpolate(h, map, th, ph);
+}
+
+// LOS geometry of the FP64 shell kernel, exposed for known-answer tests.
+__global__ void los_geometry_kernel(uint64_t n, const double *theta,
+                                    const double *phi, const double *b,
+                                    double *versor, double *b_par,
+                                    double *b_per, double *c2ipa,
+                                    double *s2ipa) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double th = theta[i], ph = phi[i];
+  const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
+  const double ux = cp * st, uy = sp * st, uz = ct;
+  const double bx = b[3 * i], by = b[3 * i + 1], bz = b[3 * i + 2];
+  versor[3 * i] = ux;
+  versor[3 * i + 1] = uy;
+  versor[3 * i + 2] = uz;
+  b_par[i] = bx * ux + by * uy + bz * uz;
+  const double cx = by * uz - bz * uy, cy = bz * ux - bx * uz,
+               cz = bx * uy - by * ux;
+  b_per[i] = sqrt(cx * cx + cy * cy + cz * cz);
+  double c2, s2;
+  ipa2<double>(-(-sp * bx + cp * by), -(ct * cp * bx + ct * sp * by - st * bz),
+               c2, s2);
+  c2ipa[i] = c2;
+  s2ipa[i] = s2;
+}
+
+// Trilinear read of one packed group at n positions (working units in,
+// working units out: 3 B components then n_e per position).
+template <typename T>
+__global__ void read_group_kernel(DevGridGroup g, uint64_t n,
+                                  const double *pos, double *out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  CellCache<T> cc;
+  cc.key = -1;
+  T b[3] = {T(0), T(0), T(0)};
+  T te = T(0);
+  sample_group<T, false>(g, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], cc, b,
+                         te);
+  out[4 * i] = b[0];
+  out[4 * i + 1] = b[1];
+  out[4 * i + 2] = b[2];
+  out[4 * i + 3] = te;
+}
+
+// Pack the FP64 SoA slots of one geometry into 4-component voxel records:
+// rec = {sum of B slots (x,y,z), sum of n_e slots}, scaled by bscale / tscale.
+template <typename T>
+__global__ void pack_kernel(uint64_t n, T *rec, const double *bx0,
+                            const double *by0, const double *bz0,
+                            const double *bx1, const double *by1,
+                            const double *bz1, const double *t0,
+                            const double *t1, double bscale, double tscale) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double bx = 0., by = 0., bz = 0., te = 0.;
+  if (bx0) {
+    bx = bx0[i];
+    by = by0[i];
+    bz = bz0[i];
+  }
+  if (bx1) {
+    bx += bx1[i];
+    by += by1[i];
+    bz += bz1[i];
+  }
+  if (t0) te = t0[i];
+  if (t1) te += t1[i];
+  rec[4 * i] = T(bx * bscale);
+  rec[4 * i + 1] = T(by * bscale);
+  rec[4 * i + 2] = T(bz * bscale);
+  rec[4 * i + 3] = T(te * tscale);
+}
+
+// ---- launch wrappers -----------------------------------------------------
+static inline unsigned blocks_for(uint64_t n, unsigned tpb) {
+  return (unsigned)((n + tpb - 1) / tpb);
+}
+
+cudaError_t launch_accumulate(cudaStream_t s, int nside_dst, int nside_src,
+                              int nmaps, double *const *dst,
+                              const double *const *src) {
+  const uint64_t n = 12ull * nside_dst * nside_dst;
+  accumulate_kernel<<<blocks_for(n, 256), 256, 0, s>>>(
+      nside_dst, nside_src, nmaps, dst[0], src[0], nmaps > 1 ? dst[1] : nullptr,
+      nmaps > 1 ? src[1] : nullptr, nmaps > 2 ? dst[2] : nullptr,
+      nmaps > 2 ? src[2] : nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pix2ang(cudaStream_t s, int nside, uint64_t n,
+                           double *theta, double *phi) {
+  pix2ang_kernel<<<blocks_for(n, 256), 256, 0, s>>>(nside, n, theta, phi);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_interpolate(cudaStream_t s, int nside, const double *map,
+                               uint64_t n, const double *theta,
+                               const double *phi, double *out) {
+  interpolate_kernel<<<blocks_for(n, 256), 256, 0, s>>>(nside, map, n, theta,
+                                                        phi, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_los_geometry(cudaStream_t s, uint64_t n,
+                                const double *theta, const double *phi,
+                                const double *b, double *versor, double *bpar,
+                                double *bper, double *c2, double *s2) {
+  los_geometry_kernel<<<blocks_for(n, 256), 256, 0, s>>>(
+      n, theta, phi, b, versor, bpar, bper, c2, s2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_read_group(cudaStream_t s, bool fp32,
+                              const DevGridGroup &g, uint64_t n,
+                              const double *pos, double *out) {
+  if (fp32)
+    read_group_kernel<float><<<blocks_for(n, 256), 256, 0, s>>>(g, n, pos, out);
+  else
+    read_group_kernel<double><<<blocks_for(n, 256), 256, 0, s>>>(g, n, pos, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack(cudaStream_t s, bool fp32, uint64_t n, void *rec,
+                        const double *const b0[3], const double *const b1[3],
+                        const double *t0, const double *t1, double bscale,
+                        double tscale) {
+  if (fp32)
+    pack_kernel<float><<<blocks_for(n, 256), 256, 0, s>>>(
+        n, static_cast<float *>(rec), b0[0], b0[1], b0[2], b1[0], b1[1], b1[2],
+        t0, t1, bscale, tscale);
+  else
+    pack_kernel<double><<<blocks_for(n, 256), 256, 0, s>>>(
+        n, static_cast<double *>(rec), b0[0], b0[1], b0[2], b1[0], b1[1],
+        b1[2], t0, t1, bscale, tscale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shell(cudaStream_t s, bool fp32, const ShellLaunch &P,
+                         unsigned blocks, unsigned threads) {
+  const int ng = P.ngroups;
+  if (fp32) {
+    if (ng == 0)
+      shell_fp32c_kernel<0, false><<<blocks, threads, 0, s>>>(P);
+    else if (ng == 1)
+      shell_fp32c_kernel<1, true><<<blocks, threads, 0, s>>>(P);
+    else
+      shell_fp32c_kernel<4, false><<<blocks, threads, 0, s>>>(P);
+  } else {
+    if (ng == 0)
+      shell_fp64_kernel<0, false><<<blocks, threads, 0, s>>>(P);
+    else if (ng == 1)
+      shell_fp64_kernel<1, true><<<blocks, threads, 0, s>>>(P);
+    else
+      shell_fp64_kernel<4, false><<<blocks, threads, 0, s>>>(P);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace hxg

@@ -1,0 +1,183 @@
+"""Python face of the B200 integrator: the reference's
+Integrator::write_grid (source/integrator/integrator.cc:23-134) over the C ABI.
+
+    integ = Integrator(precision="fp64")          # or "fp32c"
+    integ.set_models(models)                      # abi.Models
+    integ.upload_grid(abi.HXG_FIELD_BRND, desc, [bx, by, bz])
+    maps = integ.write_grid(obs)                  # dict dm/fd/is/qs/us (numpy)
+
+Device-resident inputs and outputs (torch CUDA tensors) go through
+``upload_grid_device`` and ``write_grid_device``.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib, abi
+
+PRECISIONS = {"fp64": abi.HXG_FP64, "fp32c": abi.HXG_FP32C}
+
+
+class Integrator:
+    def __init__(self, precision="fp64", device=0):
+        self._lib = _lib.load()
+        self.precision = precision
+        h = C.c_void_p()
+        _lib.check(self._lib.hxg_create(int(device), PRECISIONS[precision], C.byref(h)))
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.hxg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- configuration -------------------------------------------------
+    def set_models(self, models):
+        _lib.check(self._lib.hxg_set_models(self._h, C.byref(models)), self._h)
+
+    def set_stream(self, stream_ptr):
+        """Launch on a CUDA stream (integer cudaStream_t, e.g.
+        torch.cuda.current_stream().cuda_stream); 0 = the handle's own."""
+        _lib.check(self._lib.hxg_set_stream(self._h, C.c_void_p(stream_ptr or None)), self._h)
+
+    def upload_grid(self, field, desc, comps):
+        """Host FP64 SoA arrays in the Grid_* layout (x-major, z fastest)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in comps]
+        ptrs = [_lib.dptr(a) for a in arrs] + [None] * (3 - len(arrs))
+        _lib.check(self._lib.hxg_upload_grid(self._h, int(field), C.byref(desc), *ptrs),
+                   self._h)
+
+    def upload_grid_device(self, field, desc, comps):
+        """Device FP64 SoA arrays (torch CUDA float64 tensors, contiguous)."""
+        ptrs = [C.c_void_p(t.data_ptr()) for t in comps] + [None] * (3 - len(comps))
+        _lib.check(self._lib.hxg_upload_grid_device(self._h, int(field), C.byref(desc),
+                                                    *ptrs), self._h)
+
+    def set_mask(self, nside, mask):
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
+        _lib.check(self._lib.hxg_set_mask(self._h, int(nside), _lib.dptr(m)), self._h)
+
+    # ---- integration -----------------------------------------------------
+    def write_grid(self, obs):
+        """One frequency pass; returns the Grid_obs maps (before
+        Grid_obs::export_grid's unit rescale) as float64 numpy arrays."""
+        ndm, nfd, nsy = abi.obs_output_sizes(obs)
+        out = {"dm": np.zeros(ndm) if ndm else None,
+               "fd": np.zeros(nfd) if nfd else None,
+               "is": np.zeros(nsy) if nsy else None,
+               "qs": np.zeros(nsy) if nsy else None,
+               "us": np.zeros(nsy) if nsy else None}
+        _lib.check(self._lib.hxg_write_grid(
+            self._h, C.byref(obs), *(_lib.dptr(out[k]) for k in ("dm", "fd", "is", "qs", "us"))),
+            self._h)
+        return out
+
+    def write_grid_device(self, obs, dm=None, fd=None, is_=None, qs=None, us=None):
+        """Asynchronous variant writing into device buffers (torch CUDA
+        float64 tensors) on the handle's stream."""
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        _lib.check(self._lib.hxg_write_grid_device(
+            self._h, C.byref(obs), ptr(dm), ptr(fd), ptr(is_), ptr(qs), ptr(us)), self._h)
+
+    def sync(self):
+        _lib.check(self._lib.hxg_sync(self._h), self._h)
+
+    # ---- timing ----------------------------------------------------------
+    def set_timing(self, enable=True):
+        _lib.check(self._lib.hxg_set_timing(self._h, int(bool(enable))), self._h)
+
+    def get_timing(self):
+        ms = C.c_double()
+        n = C.c_int64()
+        s = C.c_int64()
+        _lib.check(self._lib.hxg_get_timing(self._h, C.byref(ms), C.byref(n), C.byref(s)),
+                   self._h)
+        return ms.value, n.value, s.value
+
+    def launch_count(self):
+        n = C.c_int64()
+        _lib.check(self._lib.hxg_get_launch_count(self._h, C.byref(n)), self._h)
+        return n.value
+
+    def read_grid(self, field, pos):
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+        n = len(pos) // 3
+        vec = field in (abi.HXG_FIELD_BREG, abi.HXG_FIELD_BRND)
+        out = np.zeros(3 * n if vec else n)
+        _lib.check(self._lib.hxg_read_grid(self._h, int(field), C.c_uint64(n), _lib.dptr(pos),
+                                           _lib.dptr(out)), self._h)
+        return out.reshape(n, 3) if vec else out
+
+
+# ---- stateless device helpers (known-answer entry points) -----------------
+
+def pix2ang(nside):
+    lib = _lib.load()
+    n = abi.npix(nside)
+    th, ph = np.zeros(n), np.zeros(n)
+    _lib.check(lib.hxg_pix2ang(int(nside), n, _lib.dptr(th), _lib.dptr(ph)))
+    return th, ph
+
+
+def interpolate(nside, m, theta, phi):
+    lib = _lib.load()
+    m = np.ascontiguousarray(m, dtype=np.float64)
+    theta = np.ascontiguousarray(theta, dtype=np.float64)
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    out = np.zeros(len(theta))
+    _lib.check(lib.hxg_interpolate(int(nside), _lib.dptr(m), len(theta), _lib.dptr(theta),
+                                   _lib.dptr(phi), _lib.dptr(out)))
+    return out
+
+
+def accumulate(nside_dst, dst, nside_src, src):
+    lib = _lib.load()
+    dst = np.array(dst, dtype=np.float64)
+    src = np.ascontiguousarray(src, dtype=np.float64)
+    _lib.check(lib.hxg_accumulate(int(nside_dst), _lib.dptr(dst), int(nside_src),
+                                  _lib.dptr(src)))
+    return dst
+
+
+def los_geometry(theta, phi, b):
+    lib = _lib.load()
+    theta = np.ascontiguousarray(theta, dtype=np.float64)
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1)
+    n = len(theta)
+    ver, par, per = np.zeros(3 * n), np.zeros(n), np.zeros(n)
+    c2, s2 = np.zeros(n), np.zeros(n)
+    _lib.check(lib.hxg_los_geometry(n, _lib.dptr(theta), _lib.dptr(phi), _lib.dptr(b),
+                                    _lib.dptr(ver), _lib.dptr(par), _lib.dptr(per),
+                                    _lib.dptr(c2), _lib.dptr(s2)))
+    return ver.reshape(n, 3), par, per, c2, s2
+
+
+def shell_ref(obs, shell):
+    lib = _lib.load()
+    ds, dd, st = C.c_double(), C.c_double(), C.c_uint64()
+    _lib.check(lib.hxg_shell_ref(C.byref(obs), int(shell), C.byref(ds), C.byref(dd),
+                                 C.byref(st)))
+    return ds.value, dd.value, st.value
+
+
+def mask_duplicate(pivot_nside, mask, nside):
+    lib = _lib.load()
+    mask = np.ascontiguousarray(mask, dtype=np.float64)
+    out = np.zeros(abi.npix(nside))
+    _lib.check(lib.hxg_mask_duplicate(int(pivot_nside), _lib.dptr(mask), int(nside),
+                                      _lib.dptr(out)))
+    return out

@@ -1,0 +1,292 @@
+/*
+ * hxg.h -- C ABI of the B200 line-of-sight integrator (hammurabiX hot path).
+ *
+ * One call of hxg_write_grid() is one call of the reference's
+ *   void Integrator::write_grid(const Breg*, const Brnd*, const TEreg*,
+ *        const TErnd*, const CREfield*, const Grid_breg*, const Grid_brnd*,
+ *        const Grid_tereg*, const Grid_ternd*, const Grid_cre*, Grid_obs*,
+ *        const Param*) const;                  (include/integrator.h:25-28)
+ * i.e. one frequency pass over all shells, producing the DM / FD / sync I,Q,U
+ * HEALPix RING maps that the reference accumulates into Grid_obs
+ * (source/integrator/integrator.cc:23-134).  The virtual field objects and
+ * the Param block of the reference become the plain structs below: a model
+ * enum per field slot plus the model's parameters, in the CGS units the
+ * reference's Param holds after parsing (source/param/param.cc).
+ *
+ * Conventions
+ *  - every entry point returns an int status (HXG_OK == 0); hxg_last_error()
+ *    gives the message of the last failure on a handle.  There is no CPU
+ *    fallback: without a usable CUDA device every compute call fails with
+ *    HXG_ERR_NO_DEVICE.
+ *  - all floating-point inputs and outputs are IEEE double in CGS units
+ *    (positions/lengths in cm, fields in Gauss, densities in cm^-3,
+ *    frequencies in Hz), exactly as the reference's Param and Grid_* hold
+ *    them.  Maps are HEALPix RING order, 12*nside^2 doubles.
+ *  - a handle owns one CUDA stream (or the stream given to hxg_set_stream)
+ *    and is not re-entrant; use one handle per host thread.
+ */
+#ifndef HXG_H
+#define HXG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HXG_ABI_VERSION 1
+#define HXG_MAX_SHELLS 16
+
+/* ---- status codes -------------------------------------------------------
+ * The reference throws std::runtime_error for unsupported models
+ * (source/pipeline/pipeline.cc:47,78,101,123,133,155) and asserts otherwise;
+ * the ABI returns these codes instead.                                      */
+enum {
+  HXG_OK = 0,
+  HXG_ERR_INVALID = 1,     /* bad argument, size or descriptor              */
+  HXG_ERR_UNSUPPORTED = 2, /* model / precision / combination unsupported   */
+  HXG_ERR_CUDA = 3,        /* a CUDA runtime call failed                    */
+  HXG_ERR_OOM = 4,         /* device allocation failed                      */
+  HXG_ERR_TIMEOUT = 5,     /* a bounded device wait ran out                 */
+  HXG_ERR_STATE = 6,       /* call order: e.g. grid not uploaded            */
+  HXG_ERR_NO_DEVICE = 7    /* no CUDA device / library built without one    */
+};
+
+/* ---- precision forms ---------------------------------------------------- */
+enum {
+  HXG_FP64 = 0,  /* plain FP64 everywhere (parity form)                     */
+  HXG_FP32C = 1  /* FP32 field sampling + Kahan-compensated FP32 sums; FP64
+                    for ray setup, grid coordinates, Faraday depth and its
+                    phase, and the cross-shell map sums                     */
+};
+
+/* ---- field slots (Grid_breg/brnd/tereg/ternd/cre, include/grid.h:49-168) */
+enum {
+  HXG_FIELD_BREG = 0,
+  HXG_FIELD_BRND = 1,
+  HXG_FIELD_TEREG = 2,
+  HXG_FIELD_TERND = 3,
+  HXG_FIELD_CRE = 4
+};
+
+/* ---- model enums (replace the virtual dispatch of Breg::read_field
+ *      source/field/b/breg.cc:11-26, Brnd::read_field brnd.cc:12-23,
+ *      TEreg::read_field tereg.cc:11-25, TErnd::read_field ternd.cc:12-19,
+ *      and the CREfield subclasses include/crefield.h)                     */
+enum {
+  HXG_BREG_NONE = 0,   /* Breg base class: zero field                        */
+  HXG_BREG_GRID = 1,   /* read_grid, trilinear (breg.cc:28-97)               */
+  HXG_BREG_LSA = 2,    /* Breg_lsa   (source/field/b/breg_lsa.cc:9-26)       */
+  HXG_BREG_UNIF = 3,   /* Breg_unif  (breg_unif.cc:7-12)                     */
+  HXG_BREG_CART = 4,   /* Breg_cart  (breg_cart.cc:7-11)                     */
+  HXG_BREG_HELIX = 5,  /* Breg_helix (breg_helix.cc:13-30)                   */
+  HXG_BREG_JAFFE = 6,  /* Breg_jaffe (breg_jaffe.cc)                         */
+  HXG_BREG_JF12 = 7,   /* Breg_jf12  (breg_jf12.cc)                          */
+  HXG_BREG_SPIRAL = 8  /* exponential-disk logarithmic spiral; not a
+                          reference model, defined by hxg_breg_spiral_t      */
+};
+enum { HXG_BRND_NONE = 0, HXG_BRND_GRID = 1 };
+enum {
+  HXG_TEREG_NONE = 0,
+  HXG_TEREG_GRID = 1,
+  HXG_TEREG_UNIF = 2,   /* TEreg_unif (source/field/te/tereg_unif.cc:6-12)  */
+  HXG_TEREG_YMW16 = 3,  /* TEreg_ymw16 (tereg_ymw16.cc)                     */
+  HXG_TEREG_EXPDISK = 4 /* exponential disk; not a reference model          */
+};
+enum { HXG_TERND_NONE = 0, HXG_TERND_GRID = 1 };
+enum {
+  HXG_CRE_NONE = 0,
+  HXG_CRE_ANA = 1,  /* CRE_ana  (source/field/cre/cre_ana.cc:11-63)        */
+  HXG_CRE_UNIF = 2, /* CRE_unif (cre_unif.cc:11-59)                        */
+  HXG_CRE_GRID = 3  /* CRE_num: spectral integral over a 4-D grid
+                       (integrator.cc:288-330, 357-400)                    */
+};
+
+/* ---- model parameters: field-for-field copies of Param (include/param.h) */
+typedef struct { double b0, psi0, psi1, chi0; } hxg_breg_lsa_t;   /* param.h:121-126 */
+typedef struct { double bp, bv, l0; } hxg_breg_unif_t;            /* param.h:128-131 */
+typedef struct { double bx, by, bz; } hxg_breg_cart_t;            /* param.h:149-152 */
+typedef struct { double bx, by, bz, r_min, r_max; } hxg_breg_helix_t; /* param.h:153-156 */
+typedef struct {                                                   /* param.h:133-148 */
+  int32_t quadruple, bss, ring, bar;
+  uint32_t arm_num, _pad;
+  double disk_amp, disk_z0, halo_amp, halo_z0;
+  double r_inner, r_scale, r_peak;
+  double ring_amp, bar_amp, ring_r, bar_a, bar_b, bar_phi0;
+  double arm_amp[8], arm_phi0[8];
+  double arm_pitch, arm_r0, arm_z0;
+  double comp_r, comp_c, comp_d, comp_p;
+} hxg_breg_jaffe_t;
+typedef struct {                                                   /* param.h:157-162 */
+  double b_arm1, b_arm2, b_arm3, b_arm4, b_arm5, b_arm6, b_arm7;
+  double b_ring, h_disk, w_disk;
+  double Bn, Bs, rn, rs, wh, z0;
+  double B0_X, Xtheta, rpc_X, r0_X;
+} hxg_breg_jf12_t;
+/* Exponential-disk logarithmic spiral (not in the reference):
+ *   r = sqrt(x^2+y^2); B = 0 if r > 20 kpc or r < 3 kpc, else
+ *   B = b0 * exp(-(r - r_sun)/r_scale) * exp(-|z|/h_scale)
+ *       * ( sin(pitch)cos(p) - cos(pitch)sin(p),
+ *           sin(pitch)sin(p) + cos(pitch)cos(p), 0 ),  cos(p)=x/r, sin(p)=y/r
+ * with r_sun the observer's cylindrical radius: the Breg_lsa form with
+ * psi0 = pitch, psi1 = chi0 = 0, times an exponential-disk amplitude.      */
+typedef struct { double b0, pitch, r_scale, h_scale; } hxg_breg_spiral_t;
+typedef struct { double n0, r0; } hxg_tereg_unif_t;               /* param.h:208-211 */
+/* Exponential disk (not in the reference): n = n0 exp(-r/r_scale) exp(-|z|/h_scale) */
+typedef struct { double n0, r_scale, h_scale; } hxg_tereg_expdisk_t;
+typedef struct {                                                   /* param.h:193-206 */
+  double r_warp, r0, t0_gamma_w;
+  double t1_ad, t1_bd, t1_n1, t1_h1;
+  double t2_a2, t2_b2, t2_n2, t2_k2;
+  double t3_b2s, t3_ka, t3_narm[5], t3_warm[5], t3_aa, t3_ncn, t3_wcn,
+      t3_thetacn, t3_nsg, t3_wsg, t3_thetasg, t3_rmin[5], t3_phimin[5],
+      t3_tpitch[5], t3_cpitch[5];
+  double t4_ngc, t4_agc, t4_hgc;
+  double t5_kgn, t5_ngn, t5_wgn, t5_agn;
+  double t6_j_lb, t6_nlb1, t6_detlb1, t6_wlb1, t6_hlb1, t6_thetalb1, t6_nlb2,
+      t6_detlb2, t6_wlb2, t6_hlb2, t6_thetalb2;
+  double t7_nli, t7_rli, t7_wli, t7_detthetali, t7_thetali;
+} hxg_tereg_ymw16_t;
+typedef struct { double alpha, beta, theta, r0, z0, E0, j0; } hxg_cre_ana_t; /* param.h:225-229 */
+typedef struct { double alpha, r0, E0, j0; } hxg_cre_unif_t;                 /* param.h:231-235 */
+
+typedef struct {
+  int32_t breg, brnd, tereg, ternd, cre, _pad;
+  hxg_breg_lsa_t lsa;
+  hxg_breg_unif_t unif;
+  hxg_breg_cart_t cart;
+  hxg_breg_helix_t helix;
+  hxg_breg_jaffe_t jaffe;
+  hxg_breg_jf12_t jf12;
+  hxg_breg_spiral_t spiral;
+  hxg_tereg_unif_t te_unif;
+  hxg_tereg_ymw16_t ymw16;
+  hxg_tereg_expdisk_t te_exp;
+  hxg_cre_ana_t cre_ana;
+  hxg_cre_unif_t cre_unif;
+} hxg_models_t;
+
+/* ---- grid geometry: Param::grid_{breg,brnd,tereg,ternd,cre}
+ *      (include/param.h:25-85).  Vertex grid, x-major, z fastest
+ *      (toolkit::index3d, include/toolkit.h:29-34); the CRE grid has the
+ *      energy index fastest, ((i*ny+j)*nz+k)*nE+e (source/field/cre/cre.cc:202-227). */
+typedef struct {
+  uint32_t nx, ny, nz, nE;
+  double x_min, x_max, y_min, y_max, z_min, z_max;
+  double E_min, E_max, E_fact; /* CRE only */
+} hxg_grid_desc_t;
+
+/* ---- one frequency pass: Param::grid_obs (include/param.h:87-117) ----- */
+typedef struct {
+  double observer[3];                          /* cm                        */
+  double gc_r_min, gc_r_max, gc_z_min, gc_z_max; /* cm; spherical |pos| and z */
+  double oc_r_res;                             /* cm                        */
+  uint32_t total_shell;
+  uint32_t nside_shell[HXG_MAX_SHELLS];
+  double radii_shell[HXG_MAX_SHELLS + 1];      /* cm, total_shell+1 entries */
+  int32_t do_dm, do_fd, do_sync, do_mask;
+  uint32_t nside_dm, nside_fd, nside_sync, _pad;
+  double sync_freq;                            /* Hz (sim_sync_freq.back()) */
+} hxg_obs_t;
+
+typedef struct hxg_handle hxg_handle;
+
+/* ---- library --------------------------------------------------------- */
+/* ABI version of the loaded library (HXG_ABI_VERSION at build time).      */
+int hxg_abi_version(void);
+/* Number of CUDA devices the library can see (0 without a GPU).           */
+int hxg_device_count(void);
+
+/* ---- handle lifecycle ------------------------------------------------
+ * Replaces the construction of Integrator + the upload of the Grid_*
+ * arrays that the reference reads in place (source/pipeline/pipeline.cc:23-30,
+ * 165-190).  precision is HXG_FP64 or HXG_FP32C.                         */
+int hxg_create(int device, int precision, hxg_handle **out);
+int hxg_destroy(hxg_handle *h);
+const char *hxg_last_error(const hxg_handle *h);
+/* Launch on this CUDA stream (cudaStream_t passed as void*; NULL = the
+ * handle's own stream).                                                   */
+int hxg_set_stream(hxg_handle *h, void *stream);
+
+/* ---- field models: replaces Pipeline::assemble_breg/tereg/cre model
+ *      selection (source/pipeline/pipeline.cc:33-84, 145-162).            */
+int hxg_set_models(hxg_handle *h, const hxg_models_t *m);
+
+/* ---- grids: the Grid_* SoA arrays (include/grid.h:63,94,117,144,167).
+ * field = HXG_FIELD_*; c0,c1,c2 = bx,by,bz for B slots, c0 = te for n_e
+ * slots, c0 = cre_flux for the CRE slot (c1,c2 ignored).  Host FP64; the
+ * library keeps its own device copy (FP64 and/or FP32 per precision).     */
+int hxg_upload_grid(hxg_handle *h, int field, const hxg_grid_desc_t *g,
+                    const double *c0, const double *c1, const double *c2);
+/* Same, from device-resident FP64 SoA arrays (no host copy).              */
+int hxg_upload_grid_device(hxg_handle *h, int field, const hxg_grid_desc_t *g,
+                           const double *d_c0, const double *d_c1,
+                           const double *d_c2);
+
+/* ---- mask: Grid_obs::mask_map (source/grid/grid_obs.cc:44-50) and its
+ * per-shell Hampisk::duplicate (include/hamsk.h:55-103).  A pixel is
+ * integrated iff its duplicated mask value == 1.0 (integrator.cc:69-70).
+ * mask == NULL clears it.                                                 */
+int hxg_set_mask(hxg_handle *h, uint32_t nside, const double *mask);
+
+/* ---- the integrator: Integrator::write_grid (integrator.cc:23-134) -----
+ * Outputs are the Grid_obs maps after the shell loop, before
+ * Grid_obs::export_grid's unit rescale: dm at nside_dm, fd at nside_fd,
+ * is/qs/us at nside_sync.  Pointers for observables not requested by obs
+ * may be NULL.  Host buffers; the call synchronises its stream.           */
+int hxg_write_grid(hxg_handle *h, const hxg_obs_t *obs, double *dm,
+                   double *fd, double *is, double *qs, double *us);
+/* Same with device output buffers; asynchronous on the handle's stream.   */
+int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *obs, double *d_dm,
+                          double *d_fd, double *d_is, double *d_qs,
+                          double *d_us);
+/* Wait for the handle's stream; returns the first asynchronous error.     */
+int hxg_sync(hxg_handle *h);
+
+/* ---- timing of the integration kernels ------------------------------
+ * enable != 0: every shell-integration launch is bracketed by CUDA events
+ * on the launching stream.  hxg_get_timing returns the summed device time
+ * (ms), the number of launches and the number of LOS samples they covered
+ * since the last reset.                                                   */
+int hxg_set_timing(hxg_handle *h, int enable);
+int hxg_get_timing(hxg_handle *h, double *kernel_ms, int64_t *launches,
+                   int64_t *samples);
+/* Total number of kernels this handle has launched (all kinds).          */
+int hxg_get_launch_count(hxg_handle *h, int64_t *count);
+
+/* ---- host helpers ------------------------------------------------------*/
+/* Integrator::assemble_shell_ref (integrator.cc:231-254): step count,
+ * radial step and start distance of shell `shell`.                        */
+int hxg_shell_ref(const hxg_obs_t *obs, uint32_t shell, double *d_start,
+                  double *delta_d, uint64_t *step);
+/* Hampisk::duplicate (include/hamsk.h:55-103): mask at pivot nside ->
+ * mask at nside (OR-downgrade / replicate-upgrade).                       */
+int hxg_mask_duplicate(uint32_t pivot_nside, const double *pivot_mask,
+                       uint32_t nside, double *out);
+
+/* ---- device known-answer helpers (run the kernels' own device code) ---*/
+/* Hampix fillpoint = HEALPix RING pix2ang (include/hamdis.h:302-356).     */
+int hxg_pix2ang(uint32_t nside, uint64_t npix, double *theta, double *phi);
+/* Hampix::interpolate (include/hamdis.h:609-696) of a RING map.          */
+int hxg_interpolate(uint32_t nside, const double *map, uint64_t n,
+                    const double *theta, const double *phi, double *out);
+/* Hampix::accumulate (include/hamdis.h:698-721): dst += src.              */
+int hxg_accumulate(uint32_t nside_dst, double *dst, uint32_t nside_src,
+                   const double *src);
+/* los_versor, los_parproj, los_perproj (integrator.h:35-49,
+ * integrator.cc:268-272) and cos/sin(2*sync_ipa) (integrator.cc:257-265)
+ * for n directions/fields; b is 3n doubles, versor 3n doubles.            */
+int hxg_los_geometry(uint64_t n, const double *theta, const double *phi,
+                     const double *b, double *versor, double *b_par,
+                     double *b_per, double *cos2ipa, double *sin2ipa);
+/* Trilinear read of an uploaded grid slot at n positions (3n doubles, cm):
+ * Breg/Brnd::read_grid (breg.cc:28-97, brnd.cc:25-88), TEreg/TErnd::read_grid
+ * (tereg.cc:27-74, ternd.cc:21-71).  out gets 3n (B) or n (n_e) doubles.  */
+int hxg_read_grid(hxg_handle *h, int field, uint64_t n, const double *pos,
+                  double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HXG_H */

@@ -1,0 +1,111 @@
+"""Small parity cases shared by the golden-fixture generator and the tests.
+
+Each case returns (list of Obs passes, Models, grids dict or None,
+(mask_nside, mask) or None).  Sizes are chosen so that the CPU oracle runs
+each case in about a second.
+"""
+import numpy as np
+
+from hammurabix_b200 import abi, workloads as W
+from hammurabix_b200 import units as U
+
+
+def _grid_fields(n, seeds):
+    bx, by, bz, ne = W.random_grids(n, *seeds)
+    return bx, by, bz, ne
+
+
+def case_config1():
+    """The analytic config-1 workload itself (Nside 32, 512 steps)."""
+    obs, m = W.config1()
+    return [obs], m, None, None
+
+
+def case_grid_small(fields=None):
+    """Config-2 shape, scaled down: 32^3 grids, Nside 4/8/16, 30 kpc, two
+    frequencies in the reference's Pipeline order."""
+    bx, by, bz, ne = fields if fields is not None else _grid_fields(32, (1, 2))
+    passes = W.config_grid([4, 8, 16], 30.0, 0.1, [1.4, 23.0])
+    return passes, W.grid_models(), W.grids_dict(32, bx, by, bz, ne), None
+
+
+def case_grid_lowfreq(fields=None):
+    """Strong Faraday rotation: 0.408 GHz, Nside 8/16/32 output at 32,
+    3 shells to 30 kpc."""
+    bx, by, bz, ne = fields if fields is not None else _grid_fields(32, (1, 2))
+    passes = W.config_grid([8, 16, 32], 30.0, 0.05, [0.408])
+    return passes, W.grid_models(), W.grids_dict(32, bx, by, bz, ne), None
+
+
+def case_mask(fields=None):
+    """A HEALPix mask at Nside 8 applied to Nside 4/8/16 shells."""
+    passes = W.config_grid([4, 8, 16], 20.0, 0.1, [23.0])
+    rng = np.random.Generator(np.random.PCG64(11))
+    mask = (rng.random(abi.npix(8)) > 0.3).astype(np.float64)
+    for o in passes:
+        o.do_mask = 1
+    m = W.spiral_models()
+    return passes, m, None, (8, mask)
+
+
+def case_models():
+    """One pass per analytic model of the reference (LSA, unif, cart, helix;
+    TEreg_unif; CRE_unif), Nside 8, 2 shells, DM + FD + sync 1.4 GHz."""
+    out = []
+    base = W.make_obs([8, 16], 20.0, 0.05, freq_ghz=1.4, nside_out=16)
+    def mk(breg, tereg, cre):
+        m = W.spiral_models()
+        m.breg = breg
+        m.lsa.b0 = 3.0 * U.muGauss
+        m.lsa.psi0 = 27.0 * U.rad
+        m.lsa.psi1 = 0.9 * U.rad
+        m.lsa.chi0 = 25.0 * U.rad
+        m.unif.bp = 2.0 * U.muGauss
+        m.unif.bv = 0.5 * U.muGauss
+        m.unif.l0 = 70.0 * U.rad
+        m.cart.bx = 1.0 * U.muGauss
+        m.cart.by = -0.5 * U.muGauss
+        m.cart.bz = 0.2 * U.muGauss
+        m.helix.bx = 1.0 * U.muGauss
+        m.helix.by = 1.0 * U.muGauss
+        m.helix.bz = 0.3 * U.muGauss
+        m.helix.r_min = 3.0 * U.kpc
+        m.helix.r_max = 9.0 * U.kpc
+        m.tereg = tereg
+        m.te_unif.n0 = 0.01
+        m.te_unif.r0 = 3.0 * U.kpc
+        m.cre = cre
+        m.cre_unif.alpha = 3.0
+        m.cre_unif.r0 = 3.0 * U.kpc
+        m.cre_unif.E0 = 20.6 * U.GeV
+        m.cre_unif.j0 = 0.0217
+        return m
+    combos = [
+        ("lsa", abi.HXG_BREG_LSA, abi.HXG_TEREG_EXPDISK, abi.HXG_CRE_ANA),
+        ("unif", abi.HXG_BREG_UNIF, abi.HXG_TEREG_UNIF, abi.HXG_CRE_UNIF),
+        ("cart", abi.HXG_BREG_CART, abi.HXG_TEREG_EXPDISK, abi.HXG_CRE_UNIF),
+        ("helix", abi.HXG_BREG_HELIX, abi.HXG_TEREG_EXPDISK, abi.HXG_CRE_ANA),
+        ("cre_vary", abi.HXG_BREG_SPIRAL, abi.HXG_TEREG_EXPDISK, abi.HXG_CRE_ANA),
+    ]
+    for name, b, t, c in combos:
+        m = mk(b, t, c)
+        if name == "cre_vary":
+            m.cre_ana.beta = 0.05
+            m.cre_ana.theta = 0.1
+        out.append((name, [base], m))
+    return out
+
+
+def case_dm_only():
+    """DM-only pass (no FD, no sync) with two grid geometries."""
+    o = W.make_obs([8, 16], 25.0, 0.05, freq_ghz=None, do_fd=False)
+    bx, by, bz, ne = _grid_fields(24, (5, 6))
+    g = W.grids_dict(24, bx, by, bz, ne)
+    # a second n_e grid on a different box, read as Grid_ternd
+    d2 = W.grid_desc(16, (-15.0, 15.0, -15.0, 15.0, -3.0, 3.0))
+    rng = np.random.Generator(np.random.PCG64(9))
+    ne2 = (0.01 * rng.random(16 ** 3)).astype(np.float32).astype(np.float64)
+    g[abi.HXG_FIELD_TERND] = (d2, [ne2])
+    m = W.grid_models()
+    m.ternd = abi.HXG_TERND_GRID
+    return [o], m, g, None
