@@ -224,7 +224,10 @@ def main():
     ws, rank, local = setup_dist(args)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated stream: the library launches on it and the CUDA events
+    # that time the step are recorded on it
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     n = wl["grid_n"]
     t0 = time.time()
     fields = W.random_grids_torch(n, *wl["seeds"], device=dev)
@@ -300,10 +303,14 @@ def main():
         ig64 = make_integ("fp64")
         out64 = outputs()
         step(ig64, out64)
+        ig64.set_timing(True)
         t64 = max_over_ranks(timed(ig64, out64, args.fp64_steps))
+        k64ms, _, k64s = ig64.get_timing()
+        ig64.set_timing(False)
         ms64 = t64 / args.fp64_steps * 1e3
         fp64 = {"ms_per_step": ms64, "ms_per_map": ms64 / len(passes),
-                "samples_per_s": ws * samples_step / (ms64 / 1e3)}
+                "samples_per_s": ws * samples_step / (ms64 / 1e3),
+                "kernel_samples_per_s": k64s / (k64ms / 1e3) if k64ms > 0 else None}
         # errors of the last pass (0.408 GHz, sync only) and of the first
         # pass's DM/FD: rerun pass 0 and the last pass in both forms
         errs = {}
@@ -331,18 +338,17 @@ def main():
         for p, t in zip(pinned, f64):
             p.copy_(t)
         hosts = [p.numpy() for p in pinned]
-        outs_h = [np.zeros(npx) for _ in range(5)]
+        keys = ("dm", "fd", "is", "qs", "us")
+        pinned_out = [{k: torch.empty(npx, dtype=torch.float64, pin_memory=True).numpy()
+                       for k in keys} for _ in passes]
         ige = Integrator("fp32c", device=local)
         ige.set_models(models)
 
         def e2e_step():
             ige.upload_grid(abi.HXG_FIELD_BRND, desc, hosts[:3])
             ige.upload_grid(abi.HXG_FIELD_TEREG, desc, hosts[3:])
-            for o in passes:
-                res = ige.write_grid(o)
-                for j, k in enumerate(("dm", "fd", "is", "qs", "us")):
-                    if res[k] is not None:
-                        outs_h[j] = res[k]
+            for o, po in zip(passes, pinned_out):
+                ige.write_grid(o, out=po)
 
         e2e_step()
         barrier()

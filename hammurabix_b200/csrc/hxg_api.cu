@@ -535,6 +535,7 @@ int upload_common(hxg_handle *h, int field, const hxg_grid_desc_t *g,
 
 }  // namespace
 
+
 // ============================================================ C ABI ======
 extern "C" {
 

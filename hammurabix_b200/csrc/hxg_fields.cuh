@@ -48,16 +48,42 @@ struct V3 {
   T x, y, z;
 };
 
+// Discontinuity decisions of the models.  The FP64 form takes them exactly
+// as the reference does; the FP32 form takes them on the FP64 position p so
+// that a sample next to a cutoff lands on the same side as in FP64.
+template <typename T>
+__device__ __forceinline__ bool outside_annulus(T r, const double p[3],
+                                                double kpc, double lo_kpc,
+                                                double hi_kpc) {
+  if (sizeof(T) == 8) return r > (T(hi_kpc) * T(kpc)) || r < (T(lo_kpc) * T(kpc));
+  const double r2 = p[0] * p[0] + p[1] * p[1];
+  const double hi = hi_kpc * kpc, lo = lo_kpc * kpc;
+  return r2 > hi * hi || r2 < lo * lo;
+}
+
+// |pos - observer| > r0 (tereg_unif.cc:8, cre_unif.cc:16)
+template <typename T>
+__device__ __forceinline__ bool beyond_observer(T x, T y, T z,
+                                                const double p[3],
+                                                const DevModels &m, double r0) {
+  if (sizeof(T) == 8) {
+    const T dx = x - T(m.obs[0]), dy = y - T(m.obs[1]), dz = z - T(m.obs[2]);
+    return sqrt(dx * dx + dy * dy + dz * dz) > T(r0);
+  }
+  const double dx = p[0] - m.obs[0], dy = p[1] - m.obs[1], dz = p[2] - m.obs[2];
+  return r0 < 0. || dx * dx + dy * dy + dz * dz > r0 * r0;
+}
+
 // ---- regular magnetic field models (Breg::write_field overrides) ---------
 template <typename T>
 __device__ __forceinline__ V3<T> breg_model(const DevModels &m, T x, T y,
-                                            T z) {
+                                            T z, const double p[3]) {
   V3<T> b{T(0), T(0), T(0)};
   switch (m.breg) {
     case kBregLsa: {  // breg_lsa.cc:9-26
       const T kpc = T(m.kpc);
       const T r = sqrt(x * x + y * y);
-      if (r > (T(20.) * kpc) || r < (T(3.) * kpc)) return b;
+      if (outside_annulus<T>(r, p, m.kpc, 3., 20.)) return b;
       const T cos_p = x / r, sin_p = y / r;
       const T psi = T(m.lsa_psi0) + T(m.lsa_psi1) * log(r / (T(8.) * kpc));
       const T chi = T(m.lsa_chi0) * tanh(z / (T(1.) * kpc));
@@ -77,7 +103,15 @@ __device__ __forceinline__ V3<T> breg_model(const DevModels &m, T x, T y,
     case kBregHelix: {  // breg_helix.cc:13-30
       const T r = sqrt(x * x + y * y);
       const T phi = atan2(y, x) + T(cgs::pi / 2.0);
-      if ((r > T(m.hx_rmin)) && (r < T(m.hx_rmax))) {
+      bool inside;
+      if (sizeof(T) == 8) {
+        inside = (r > T(m.hx_rmin)) && (r < T(m.hx_rmax));
+      } else {
+        const double r2 = p[0] * p[0] + p[1] * p[1];
+        inside = (m.hx_rmin < 0. || r2 > m.hx_rmin * m.hx_rmin) &&
+                 (m.hx_rmax > 0. && r2 < m.hx_rmax * m.hx_rmax);
+      }
+      if (inside) {
         b.x = T(m.hx_bx) * cos(phi);
         b.y = T(m.hx_by) * sin(phi);
         b.z = T(m.hx_bz);
@@ -85,9 +119,8 @@ __device__ __forceinline__ V3<T> breg_model(const DevModels &m, T x, T y,
       return b;
     }
     case kBregSpiral: {
-      const T kpc = T(m.kpc);
       const T r = sqrt(x * x + y * y);
-      if (r > (T(20.) * kpc) || r < (T(3.) * kpc)) return b;
+      if (outside_annulus<T>(r, p, m.kpc, 3., 20.)) return b;
       const T cos_p = x / r, sin_p = y / r;
       const T amp = T(m.sp_b0) * exp(-(r - T(m.sp_rsun)) / T(m.sp_rs)) *
                     exp(-fabs(z) / T(m.sp_hs));
@@ -103,13 +136,11 @@ __device__ __forceinline__ V3<T> breg_model(const DevModels &m, T x, T y,
 
 // ---- regular thermal-electron models (TEreg::write_field overrides) ------
 template <typename T>
-__device__ __forceinline__ T tereg_model(const DevModels &m, T x, T y, T z) {
+__device__ __forceinline__ T tereg_model(const DevModels &m, T x, T y, T z,
+                                        const double p[3]) {
   switch (m.tereg) {
-    case kTeregUnif: {  // tereg_unif.cc:6-12
-      const T dx = x - T(m.obs[0]), dy = y - T(m.obs[1]), dz = z - T(m.obs[2]);
-      const T l = sqrt(dx * dx + dy * dy + dz * dz);
-      return (l > T(m.teu_r0)) ? T(0) : T(m.teu_n0);
-    }
+    case kTeregUnif:  // tereg_unif.cc:6-12
+      return beyond_observer<T>(x, y, z, p, m, m.teu_r0) ? T(0) : T(m.teu_n0);
     case kTeregExpdisk: {
       const T r = sqrt(x * x + y * y);
       return T(m.tex_n0) * exp(-r / T(m.tex_rs)) * exp(-fabs(z) / T(m.tex_hs));
@@ -132,15 +163,14 @@ __device__ __forceinline__ T cre_index(const DevModels &m, T x, T y, T z) {
 }
 
 template <typename T>
-__device__ __forceinline__ T cre_profile(const DevModels &m, T x, T y, T z) {
+__device__ __forceinline__ T cre_profile(const DevModels &m, T x, T y, T z,
+                                        const double p[3]) {
   if (m.cre == kCreAna) {
     const T r = sqrt(x * x + y * y);
     const T ch = cosh(z / T(m.cre_z0));
     return exp((T(m.cre_R0) - r) / T(m.cre_r0)) * (T(1.) / (ch * ch));
   }
-  const T dx = x - T(m.obs[0]), dy = y - T(m.obs[1]), dz = z - T(m.obs[2]);
-  const T l = sqrt(dx * dx + dy * dy + dz * dz);
-  return (l > T(m.cre_unif_r0)) ? T(0) : T(1);
+  return beyond_observer<T>(x, y, z, p, m, m.cre_unif_r0) ? T(0) : T(1);
 }
 
 // ---- packed grid groups --------------------------------------------------

@@ -174,8 +174,9 @@ shell_fp64_kernel(const ShellLaunch P) {
       if (len < P.gc_r_min || len > P.gc_r_max || pz < P.gc_z_min ||
           pz > P.gc_z_max)
         continue;
-      V3<double> B = breg_model<double>(M, px, py, pz);
-      double te = tereg_model<double>(M, px, py, pz);
+      const double p3[3] = {px, py, pz};
+      V3<double> B = breg_model<double>(M, px, py, pz, p3);
+      double te = tereg_model<double>(M, px, py, pz, p3);
       if (NG > 0) {
         double b3[3] = {B.x, B.y, B.z};
 #pragma unroll 1
@@ -203,7 +204,7 @@ shell_fp64_kernel(const ShellLaunch P) {
             last_index = index;
           }
         }
-        const double fn = P.em_n0u * cre_profile<double>(M, px, py, pz);
+        const double fn = P.em_n0u * cre_profile<double>(M, px, py, pz, p3);
         const double absb = fabs(bper);
         const double A = P.em_anum / (P.em_3qe * absb);
         double Ae;
@@ -297,8 +298,7 @@ shell_fp32c_kernel(const ShellLaunch P) {
           gp = float(P.em_gp), inv1mi = 1.f;
     const long long i0 = (P.step * c) >> P.log2_chunks;
     const long long i1 = (P.step * (c + 1)) >> P.log2_chunks;
-    double dd = P.d_start + ((double)i0 + 0.5) * P.delta;
-    for (long long i = i0; i < i1; ++i, dd += P.delta) {
+    for (long long i = i0; i < i1; ++i) {
       const double d = P.d_start + ((double)i + 0.5) * P.delta;
       const double px = fma(ux, d, P.obs[0]);
       const double py = fma(uy, d, P.obs[1]);
@@ -307,8 +307,9 @@ shell_fp32c_kernel(const ShellLaunch P) {
       if (r2 < r2min || r2 > r2max || pz < P.gc_z_min || pz > P.gc_z_max)
         continue;
       const float x = float(px), y = float(py), z = float(pz);
-      V3<float> B = breg_model<float>(M, x, y, z);
-      float te = tereg_model<float>(M, x, y, z);
+      const double p3[3] = {px, py, pz};
+      V3<float> B = breg_model<float>(M, x, y, z, p3);
+      float te = tereg_model<float>(M, x, y, z, p3);
       if (NG > 0) {
         float b3[3] = {B.x, B.y, B.z};
 #pragma unroll 1
@@ -327,7 +328,7 @@ shell_fp32c_kernel(const ShellLaunch P) {
       if (P.do_dm) kdm.add(te);
       if (P.do_fd || P.do_sync) sfd += double(te * bpar);
       if (P.do_sync) {
-        const float prof = cre_profile<float>(M, x, y, z);
+        const float prof = cre_profile<float>(M, x, y, z, p3);
         float wt, wp;
         if (P.em_const) {
           float bp;
@@ -365,7 +366,6 @@ shell_fp32c_kernel(const ShellLaunch P) {
         ku.add(wp * (sf * c2 + cf * s2));
       }
     }
-    (void)dd;
     dm = kdm.value() * P.k_dm;
     fd = sfd * P.fd_fore;
     si = ki.value() * P.k_t;

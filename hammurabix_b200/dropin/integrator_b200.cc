@@ -1,0 +1,255 @@
+// integrator_b200.cc -- link-time drop-in for hammurabiX's integrator.
+//
+// Defines the reference's own
+//   void Integrator::write_grid(const Breg*, const Brnd*, const TEreg*,
+//                               const TErnd*, const CREfield*,
+//                               const Grid_breg*, const Grid_brnd*,
+//                               const Grid_tereg*, const Grid_ternd*,
+//                               const Grid_cre*, Grid_obs*, const Param*) const;
+// (include/integrator.h:25-28) on top of the hxg C ABI (include/hxg.h).
+// Compiled in place of source/integrator/integrator.cc and linked with
+// lib/libhxg.so, the unmodified Pipeline (source/pipeline/pipeline.cc) and
+// CLI (source/main/main_std.cc) run their line-of-sight integration on the
+// GPU.  Errors follow the reference's convention: std::runtime_error.
+//
+// Environment: HAMMURABIX_PRECISION = fp64 (default) | fp32c,
+//              HAMMURABIX_DEVICE = CUDA device index (default 0).
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <typeinfo>
+#include <vector>
+
+#include <bfield.h>
+#include <crefield.h>
+#include <grid.h>
+#include <hamdis.h>
+#include <hamsk.h>
+#include <integrator.h>
+#include <param.h>
+#include <tefield.h>
+
+#include "../../include/hxg.h"
+
+namespace {
+
+void check(int st, hxg_handle *h, const char *what) {
+  if (st != HXG_OK) {
+    std::string msg = std::string("hammurabiX-B200: ") + what + " failed (status " +
+                      std::to_string(st) + ")";
+    if (h) msg += std::string(": ") + hxg_last_error(h);
+    throw std::runtime_error(msg);
+  }
+}
+
+// One device handle per process, re-used across frequency passes
+// (Pipeline::assemble_obs calls write_grid once per <sync> entry).
+struct DeviceState {
+  hxg_handle *h = nullptr;
+  const void *uploaded[4] = {nullptr, nullptr, nullptr, nullptr};
+  ~DeviceState() {
+    if (h) hxg_destroy(h);
+  }
+};
+
+DeviceState &state() {
+  static DeviceState s;
+  if (!s.h) {
+    const char *p = std::getenv("HAMMURABIX_PRECISION");
+    const int prec = (p && std::string(p) == "fp32c") ? HXG_FP32C : HXG_FP64;
+    const char *d = std::getenv("HAMMURABIX_DEVICE");
+    check(hxg_create(d ? std::atoi(d) : 0, prec, &s.h), nullptr, "hxg_create");
+  }
+  return s;
+}
+
+template <typename P>
+hxg_grid_desc_t desc_of(const P &g) {
+  hxg_grid_desc_t d{};
+  d.nx = static_cast<uint32_t>(g.nx);
+  d.ny = static_cast<uint32_t>(g.ny);
+  d.nz = static_cast<uint32_t>(g.nz);
+  d.x_min = g.x_min;
+  d.x_max = g.x_max;
+  d.y_min = g.y_min;
+  d.y_max = g.y_max;
+  d.z_min = g.z_min;
+  d.z_max = g.z_max;
+  return d;
+}
+
+void upload_vec(DeviceState &s, int slot, const hxg_grid_desc_t &d,
+                const double *x, const double *y, const double *z) {
+  if (s.uploaded[slot] == x) return;
+  check(hxg_upload_grid(s.h, slot, &d, x, y, z), s.h, "hxg_upload_grid");
+  s.uploaded[slot] = x;
+}
+
+// The reference's model selection, read back from the field objects'
+// dynamic types and Param's permissions (pipeline.cc:33-162,
+// breg.cc:11-26, brnd.cc:12-23, tereg.cc:11-25, ternd.cc:12-19).
+hxg_models_t map_models(DeviceState &s, const Breg *breg, const Brnd *,
+                        const TEreg *tereg, const TErnd *, const CREfield *cre,
+                        const Grid_breg *gbreg, const Grid_brnd *gbrnd,
+                        const Grid_tereg *gtereg, const Grid_ternd *gternd,
+                        const Param *par) {
+  hxg_models_t m{};
+  // regular B
+  if (par->grid_breg.read_permission) {
+    m.breg = HXG_BREG_GRID;
+    upload_vec(s, HXG_FIELD_BREG, desc_of(par->grid_breg), gbreg->bx.get(),
+               gbreg->by.get(), gbreg->bz.get());
+  } else if (par->grid_breg.build_permission) {
+    if (dynamic_cast<const Breg_lsa *>(breg)) {
+      m.breg = HXG_BREG_LSA;
+      m.lsa = {par->breg_lsa.b0, par->breg_lsa.psi0, par->breg_lsa.psi1,
+               par->breg_lsa.chi0};
+    } else if (dynamic_cast<const Breg_unif *>(breg)) {
+      m.breg = HXG_BREG_UNIF;
+      m.unif = {par->breg_unif.bp, par->breg_unif.bv, par->breg_unif.l0};
+    } else if (dynamic_cast<const Breg_cart *>(breg)) {
+      m.breg = HXG_BREG_CART;
+      m.cart = {par->breg_cart.bx, par->breg_cart.by, par->breg_cart.bz};
+    } else if (dynamic_cast<const Breg_helix *>(breg)) {
+      m.breg = HXG_BREG_HELIX;
+      m.helix = {par->breg_helix.bx, par->breg_helix.by, par->breg_helix.bz,
+                 par->breg_helix.r_min, par->breg_helix.r_max};
+    } else if (typeid(*breg) == typeid(Breg)) {
+      m.breg = HXG_BREG_NONE;
+    } else {
+      throw std::runtime_error("hammurabiX-B200: unsupported breg model");
+    }
+  } else {
+    m.breg = HXG_BREG_NONE;
+  }
+  // random B: read_grid whenever read or build permission (brnd.cc:12-23)
+  if (par->grid_brnd.read_permission or par->grid_brnd.build_permission) {
+    m.brnd = HXG_BRND_GRID;
+    upload_vec(s, HXG_FIELD_BRND, desc_of(par->grid_brnd), gbrnd->bx.get(),
+               gbrnd->by.get(), gbrnd->bz.get());
+  }
+  // regular n_e
+  if (par->grid_tereg.read_permission) {
+    m.tereg = HXG_TEREG_GRID;
+    if (s.uploaded[HXG_FIELD_TEREG] != gtereg->te.get()) {
+      const hxg_grid_desc_t d = desc_of(par->grid_tereg);
+      check(hxg_upload_grid(s.h, HXG_FIELD_TEREG, &d, gtereg->te.get(), nullptr, nullptr),
+            s.h, "hxg_upload_grid");
+      s.uploaded[HXG_FIELD_TEREG] = gtereg->te.get();
+    }
+  } else if (par->grid_tereg.build_permission) {
+    if (dynamic_cast<const TEreg_unif *>(tereg)) {
+      m.tereg = HXG_TEREG_UNIF;
+      m.te_unif = {par->tereg_unif.n0, par->tereg_unif.r0};
+    } else if (dynamic_cast<const TEreg_ymw16 *>(tereg)) {
+      m.tereg = HXG_TEREG_YMW16;
+      static_assert(sizeof(par->tereg_ymw16) == sizeof(m.ymw16), "ymw16 layout");
+      std::memcpy(&m.ymw16, &par->tereg_ymw16, sizeof(m.ymw16));
+    } else if (typeid(*tereg) == typeid(TEreg)) {
+      m.tereg = HXG_TEREG_NONE;
+    } else {
+      throw std::runtime_error("hammurabiX-B200: unsupported tereg model");
+    }
+  }
+  // random n_e (ternd.cc:12-19)
+  if (par->grid_ternd.read_permission or par->grid_ternd.build_permission) {
+    m.ternd = HXG_TERND_GRID;
+    if (s.uploaded[HXG_FIELD_TERND] != gternd->te.get()) {
+      const hxg_grid_desc_t d = desc_of(par->grid_ternd);
+      check(hxg_upload_grid(s.h, HXG_FIELD_TERND, &d, gternd->te.get(), nullptr, nullptr),
+            s.h, "hxg_upload_grid");
+      s.uploaded[HXG_FIELD_TERND] = gternd->te.get();
+    }
+  }
+  // cosmic-ray electrons
+  if (par->grid_cre.read_permission) {
+    throw std::runtime_error("hammurabiX-B200: CRE grids are not supported on the GPU");
+  } else if (dynamic_cast<const CRE_ana *>(cre)) {
+    m.cre = HXG_CRE_ANA;
+    m.cre_ana = {par->cre_ana.alpha, par->cre_ana.beta, par->cre_ana.theta,
+                 par->cre_ana.r0,    par->cre_ana.z0,   par->cre_ana.E0,
+                 par->cre_ana.j0};
+  } else if (dynamic_cast<const CRE_unif *>(cre)) {
+    m.cre = HXG_CRE_UNIF;
+    m.cre_unif = {par->cre_unif.alpha, par->cre_unif.r0, par->cre_unif.E0,
+                  par->cre_unif.j0};
+  } else if (cre != nullptr) {
+    throw std::runtime_error("hammurabiX-B200: unsupported cre model");
+  }
+  return m;
+}
+
+hxg_obs_t map_obs(const Param *par) {
+  const auto &go = par->grid_obs;
+  hxg_obs_t o{};
+  for (int i = 0; i < 3; ++i) o.observer[i] = par->observer[i];
+  o.gc_r_min = go.gc_r_min;
+  o.gc_r_max = go.gc_r_max;
+  o.gc_z_min = go.gc_z_min;
+  o.gc_z_max = go.gc_z_max;
+  o.oc_r_res = go.oc_r_res;
+  if (go.total_shell > HXG_MAX_SHELLS)
+    throw std::runtime_error("hammurabiX-B200: too many shells");
+  o.total_shell = static_cast<uint32_t>(go.total_shell);
+  for (ham_uint s = 0; s < go.total_shell; ++s) {
+    o.nside_shell[s] = static_cast<uint32_t>(go.nside_shell[s]);
+    o.radii_shell[s] = go.radii_shell[s];
+  }
+  o.radii_shell[go.total_shell] = go.radii_shell[go.total_shell];
+  o.do_dm = go.do_dm;
+  o.do_fd = go.do_fd;
+  o.do_sync = go.do_sync.back();
+  o.do_mask = go.do_mask;
+  o.nside_dm = static_cast<uint32_t>(go.nside_dm);
+  o.nside_fd = static_cast<uint32_t>(go.nside_fd);
+  if (o.do_sync) {
+    o.nside_sync = static_cast<uint32_t>(go.nside_sync.back());
+    o.sync_freq = go.sim_sync_freq.back();
+  }
+  return o;
+}
+
+void store(Hampix<ham_float> &map, const std::vector<double> &v) {
+  for (ham_uint i = 0; i < map.npix(); ++i) map.data(i, v[i]);
+}
+
+}  // namespace
+
+void Integrator::write_grid(const Breg *breg, const Brnd *brnd,
+                            const TEreg *tereg, const TErnd *ternd,
+                            const CREfield *cre, const Grid_breg *gbreg,
+                            const Grid_brnd *gbrnd, const Grid_tereg *gtereg,
+                            const Grid_ternd *gternd, const Grid_cre *,
+                            Grid_obs *gobs, const Param *par) const {
+  DeviceState &s = state();
+  const hxg_models_t m = map_models(s, breg, brnd, tereg, ternd, cre, gbreg, gbrnd,
+                                    gtereg, gternd, par);
+  check(hxg_set_models(s.h, &m), s.h, "hxg_set_models");
+  const hxg_obs_t o = map_obs(par);
+  if (o.do_mask) {
+    const ham_uint ns = par->grid_obs.nside_mask;
+    std::vector<double> mk(12ull * ns * ns);
+    for (ham_uint i = 0; i < mk.size(); ++i) mk[i] = gobs->mask_map->data(ns, i);
+    check(hxg_set_mask(s.h, static_cast<uint32_t>(ns), mk.data()), s.h, "hxg_set_mask");
+  } else {
+    check(hxg_set_mask(s.h, 0, nullptr), s.h, "hxg_set_mask");
+  }
+  const auto npix = [](uint32_t n) { return static_cast<size_t>(12ull * n * n); };
+  std::vector<double> dm(o.do_dm ? npix(o.nside_dm) : 0), fd(o.do_fd ? npix(o.nside_fd) : 0);
+  const size_t ns = o.do_sync ? npix(o.nside_sync) : 0;
+  std::vector<double> is(ns), qs(ns), us(ns);
+  check(hxg_write_grid(s.h, &o, dm.data(), fd.data(), is.data(), qs.data(), us.data()), s.h,
+        "hxg_write_grid");
+  // Grid_obs maps are freshly built zero maps; the shell sums land in them
+  // exactly as the reference's accumulate() calls leave them.
+  if (o.do_dm) store(*gobs->dm_map, dm);
+  if (o.do_fd) store(*gobs->fd_map, fd);
+  if (o.do_sync) {
+    store(*gobs->is_map, is);
+    store(*gobs->qs_map, qs);
+    store(*gobs->us_map, us);
+  }
+}

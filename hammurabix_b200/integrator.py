@@ -71,15 +71,17 @@ class Integrator:
         _lib.check(self._lib.hxg_set_mask(self._h, int(nside), _lib.dptr(m)), self._h)
 
     # ---- integration -----------------------------------------------------
-    def write_grid(self, obs):
+    def write_grid(self, obs, out=None):
         """One frequency pass; returns the Grid_obs maps (before
-        Grid_obs::export_grid's unit rescale) as float64 numpy arrays."""
+        Grid_obs::export_grid's unit rescale) as float64 numpy arrays.
+        ``out`` may supply the destination arrays (dict dm/fd/is/qs/us of
+        C-contiguous float64 arrays of the right sizes, e.g. pinned memory)."""
         ndm, nfd, nsy = abi.obs_output_sizes(obs)
-        out = {"dm": np.zeros(ndm) if ndm else None,
-               "fd": np.zeros(nfd) if nfd else None,
-               "is": np.zeros(nsy) if nsy else None,
-               "qs": np.zeros(nsy) if nsy else None,
-               "us": np.zeros(nsy) if nsy else None}
+        sizes = {"dm": ndm, "fd": nfd, "is": nsy, "qs": nsy, "us": nsy}
+        if out is None:
+            out = {k: (np.zeros(n) if n else None) for k, n in sizes.items()}
+        else:
+            out = {k: (out[k][:n] if n else None) for k, n in sizes.items()}
         _lib.check(self._lib.hxg_write_grid(
             self._h, C.byref(obs), *(_lib.dptr(out[k]) for k in ("dm", "fd", "is", "qs", "us"))),
             self._h)
