@@ -32,6 +32,9 @@ SIGNATURES = {
     "hxg_set_timing": (C.c_int, [_h, C.c_int]),
     "hxg_get_timing": (C.c_int, [_h, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "hxg_get_launch_count": (C.c_int, [_h, C.POINTER(C.c_int64)]),
+    "hxg_write_grid_noalloc": (C.c_int, [C.POINTER(abi.Obs), C.POINTER(abi.Models),
+                                         C.POINTER(abi.GridDesc), _vp, _vp, _vp, _vp, _vp,
+                                         _vp, _vp]),
     "hxg_shell_ref": (C.c_int, [C.POINTER(abi.Obs), C.c_uint32, _dp, _dp,
                                 C.POINTER(C.c_uint64)]),
     "hxg_mask_duplicate": (C.c_int, [C.c_uint32, _dp, C.c_uint32, _dp]),

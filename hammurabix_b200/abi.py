@@ -17,11 +17,13 @@ HXG_ERR_OOM = 4
 HXG_ERR_TIMEOUT = 5
 HXG_ERR_STATE = 6
 HXG_ERR_NO_DEVICE = 7
+HXG_ERR_TOO_LARGE = 8
+HXG_NOALLOC_MAX_NSIDE = 128
 
 STATUS_NAMES = {
     0: "HXG_OK", 1: "HXG_ERR_INVALID", 2: "HXG_ERR_UNSUPPORTED",
     3: "HXG_ERR_CUDA", 4: "HXG_ERR_OOM", 5: "HXG_ERR_TIMEOUT",
-    6: "HXG_ERR_STATE", 7: "HXG_ERR_NO_DEVICE",
+    6: "HXG_ERR_STATE", 7: "HXG_ERR_NO_DEVICE", 8: "HXG_ERR_TOO_LARGE",
 }
 
 # precision forms

@@ -536,6 +536,43 @@ int upload_common(hxg_handle *h, int field, const hxg_grid_desc_t *g,
 }  // namespace
 
 
+namespace hxg {
+// Launch constants of shell s for the FP64 form from plain inputs (one
+// caller-packed grid group of FP64 records, or none), without a live handle
+// and without any allocation.  Used by the allocation-free entry point.
+int noalloc_shell_launch(const hxg_obs_t *o, const hxg_models_t *m,
+                         const hxg_grid_desc_t *g, const double *rec,
+                         uint32_t s, ShellLaunch *P, uint64_t *step) {
+  hxg_handle h;
+  h.precision = HXG_FP64;
+  h.models = *m;
+  h.have_models = true;
+  h.groups_dirty = false;
+  if (rec != nullptr) {
+    h.groups.emplace_back();
+    Group &G = h.groups.back();
+    G.desc = *g;
+    G.rec = const_cast<double *>(rec);
+    G.n = (size_t)g->nx * g->ny * g->nz;
+    G.b_slots[0] = (m->breg == HXG_BREG_GRID || m->brnd == HXG_BRND_GRID) ? 0 : -1;
+    G.t_slots[0] = (m->tereg == HXG_TEREG_GRID || m->ternd == HXG_TERND_GRID) ? 2 : -1;
+  }
+  const int st = build_launch(&h, *o, s, *P, *step);
+  h.groups.clear();  // the records belong to the caller
+  return st;
+}
+
+bool noalloc_models_supported(const hxg_models_t *m) {
+  std::string why;
+  return models_supported(*m, &why);
+}
+
+bool noalloc_obs_valid(const hxg_obs_t *o) {
+  hxg_handle h;
+  return validate_obs(&h, o) == HXG_OK;
+}
+}  // namespace hxg
+
 // ============================================================ C ABI ======
 extern "C" {
 

@@ -50,7 +50,9 @@ enum {
   HXG_ERR_OOM = 4,         /* device allocation failed                      */
   HXG_ERR_TIMEOUT = 5,     /* a bounded device wait ran out                 */
   HXG_ERR_STATE = 6,       /* call order: e.g. grid not uploaded            */
-  HXG_ERR_NO_DEVICE = 7    /* no CUDA device / library built without one    */
+  HXG_ERR_NO_DEVICE = 7,   /* no CUDA device / library built without one    */
+  HXG_ERR_TOO_LARGE = 8    /* request exceeds the fixed scratch of
+                              hxg_write_grid_noalloc                         */
 };
 
 /* ---- precision forms ---------------------------------------------------- */
@@ -254,6 +256,36 @@ int hxg_get_timing(hxg_handle *h, double *kernel_ms, int64_t *launches,
                    int64_t *samples);
 /* Total number of kernels this handle has launched (all kinds).          */
 int hxg_get_launch_count(hxg_handle *h, int64_t *count);
+
+/* ---- allocation-free integration ---------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate
+ * device memory -- code running during CUDA graph capture, plugins whose
+ * host application owns every device allocation, pipelines that must not
+ * touch the allocator after start-up -- this entry point runs the FP64
+ * integrator without any cudaMalloc/cudaFree.  Inputs and outputs are the
+ * caller's device buffers; the only scratch (the per-shell HEALPix maps) is
+ * a fixed static device array of 5 x 12 x HXG_NOALLOC_MAX_NSIDE^2 doubles
+ * (7.5 MiB) that every GPU loading the library holds until exit.
+ *
+ *  - grid / d_records: one packed grid of FP64 voxel records
+ *    {bx, by, bz, ne} (32 B per voxel, x-major, z fastest), holding the sum
+ *    of all gridded B slots and of all gridded n_e slots the models read;
+ *    NULL when the models read no grid.
+ *  - shells larger than HXG_NOALLOC_MAX_NSIDE return HXG_ERR_TOO_LARGE;
+ *    masks (do_mask) return HXG_ERR_UNSUPPORTED.
+ *  - work is queued on `stream` (cudaStream_t; NULL = legacy default) of
+ *    the current device; the call does not synchronise.
+ *  - the first call on a device looks the scratch address up on that
+ *    device (cudaGetSymbolAddress); make that first call before any stream
+ *    capture.  All calls share the scratch and it keeps the last call's
+ *    contents; calls whose GPU work overlaps (other streams, other threads)
+ *    race on it, so serialise them.                                        */
+#define HXG_NOALLOC_MAX_NSIDE 128
+int hxg_write_grid_noalloc(const hxg_obs_t *obs, const hxg_models_t *models,
+                           const hxg_grid_desc_t *grid,
+                           const double *d_records, double *d_dm,
+                           double *d_fd, double *d_is, double *d_qs,
+                           double *d_us, void *stream);
 
 /* ---- host helpers ------------------------------------------------------*/
 /* Integrator::assemble_shell_ref (integrator.cc:231-254): step count,
