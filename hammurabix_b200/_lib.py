@@ -35,6 +35,9 @@ SIGNATURES = {
     "hxg_write_grid_noalloc": (C.c_int, [C.POINTER(abi.Obs), C.POINTER(abi.Models),
                                          C.POINTER(abi.GridDesc), _vp, _vp, _vp, _vp, _vp,
                                          _vp, _vp]),
+    "hxg_set_checkpointing": (C.c_int, [_h, C.c_int]),
+    "hxg_adjoint_device": (C.c_int, [_h, C.POINTER(abi.Obs), _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                     _vp, _vp, _vp]),
     "hxg_shell_ref": (C.c_int, [C.POINTER(abi.Obs), C.c_uint32, _dp, _dp,
                                 C.POINTER(C.c_uint64)]),
     "hxg_mask_duplicate": (C.c_int, [C.c_uint32, _dp, C.c_uint32, _dp]),

@@ -153,3 +153,8 @@ def obs_output_sizes(obs):
     return (npix(obs.nside_dm) if obs.do_dm else 0,
             npix(obs.nside_fd) if obs.do_fd else 0,
             npix(obs.nside_sync) if obs.do_sync else 0)
+
+# adjoint parameter slots (include/hxg.h HXG_PARAM_*)
+HXG_PARAM_SPIRAL_B0, HXG_PARAM_SPIRAL_PITCH, HXG_PARAM_SPIRAL_R, HXG_PARAM_SPIRAL_H, \
+    HXG_PARAM_EXPDISK_N0, HXG_PARAM_EXPDISK_R, HXG_PARAM_EXPDISK_H, HXG_PARAM_CRE_J0 = range(8)
+HXG_NUM_PARAMS = 8

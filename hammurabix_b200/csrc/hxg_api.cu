@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/hxg.h"
+#include "hxg_adjoint.cuh"
 #include "hxg_integrate.cuh"
 #include "hxg_internal.h"
 
@@ -71,6 +72,14 @@ struct hxg_handle {
   int64_t acc_launches = 0, acc_samples = 0;
   double waves = 4.0;
   int64_t launch_count = 0;
+  // adjoint checkpoint of the last forward pass (FP64 form)
+  bool checkpoint = false;
+  bool ck_valid = false;
+  hxg_obs_t ck_obs{};
+  hxg_models_t ck_models{};
+  std::vector<DevBuf> ck, ck_inner;
+  std::vector<int> ck_chunks;
+  DevBuf grad_rec, grad_par, g_shell[5], g_fdmap;
 };
 
 namespace {
@@ -209,7 +218,7 @@ int build_groups(hxg_handle *h) {
       for (int k = 0; k < 3; ++k) b1[k] = h->slots[g.b_slots[1]].d[k];
     const double *t0 = g.t_slots[0] >= 0 ? h->slots[g.t_slots[0]].d[0] : nullptr;
     const double *t1 = g.t_slots[1] >= 0 ? h->slots[g.t_slots[1]].d[0] : nullptr;
-    const double bscale = fp32 ? 1.0 / cgs::muGauss : 1.0;
+    const double bscale = fp32 ? 1.0 / cgs::fp32_bunit : 1.0;
     HXG_CK(launch_pack(h->stream, fp32, g.n, g.rec, b0, b1, t0, t1, bscale, 1.0));
     ++h->launch_count;
   }
@@ -299,7 +308,7 @@ double cre_index_at(const hxg_models_t &m, const double p[3]) {
 }
 
 // Fill the model block in the working units of the form: CGS for FP64,
-// kpc / muGauss for FP32C (L = length scale, Bu = field scale).
+// kpc / 2^-20 G for FP32C (L = length scale, Bu = field scale).
 DevModels dev_models(const hxg_models_t &m, const double obs[3], double L,
                      double Bu) {
   DevModels d{};
@@ -367,7 +376,7 @@ int build_launch(hxg_handle *h, const hxg_obs_t &o, uint32_t s,
                  ShellLaunch &P, uint64_t &step_out) {
   const bool fp32 = h->precision == HXG_FP32C;
   const double L = fp32 ? 1.0 / cgs::kpc : 1.0;
-  const double Bu = fp32 ? 1.0 / cgs::muGauss : 1.0;
+  const double Bu = fp32 ? 1.0 / cgs::fp32_bunit : 1.0;
   const hxg_models_t &m = h->models;
   std::memset(&P, 0, sizeof(P));
   double d_start, delta;
@@ -415,9 +424,9 @@ int build_launch(hxg_handle *h, const hxg_obs_t &o, uint32_t s,
     P.em_3qe = 3. * qe;
     P.em_den_p = 16. * cgs::pi * mec2;
     P.em_const = P.models.cre_const_index;
-    const double a_s = P.em_anum / (P.em_3qe * cgs::muGauss);
+    const double a_s = P.em_anum / (P.em_3qe * cgs::fp32_bunit);
     P.a_s = a_s;
-    const double kbase = P.em_n0u * 1.73205081 * P.em_qe3 * cgs::muGauss;
+    const double kbase = P.em_n0u * 1.73205081 * P.em_qe3 * cgs::fp32_bunit;
     if (P.em_const) {
       const double idx =
           m.cre == HXG_CRE_ANA ? -m.cre_ana.alpha : -(m.cre_unif.alpha);
@@ -437,9 +446,20 @@ int build_launch(hxg_handle *h, const hxg_obs_t &o, uint32_t s,
     }
   }
   if (fp32) {
-    P.fd_fore = fdfore * delta * cgs::muGauss;
+    P.fd_fore = fdfore * delta * cgs::fp32_bunit;
     P.k_dm = delta;
     P.phase_k = 2. * P.lambda2 * P.fd_fore;
+    const DevModels &D = P.models;
+    FastModels &F = P.fast;
+    F.sp_b0 = D.sp_b0;
+    F.sp_irs = 1. / D.sp_rs;
+    F.sp_crs = D.sp_rsun / D.sp_rs;
+    F.sp_ihs = 1. / D.sp_hs;
+    F.sp_sin = D.sp_sin;
+    F.sp_cos = D.sp_cos;
+    F.ex_n0 = D.tex_n0;
+    F.ex_irn = 1. / D.tex_rs;
+    F.ex_ihn = 1. / D.tex_hs;
   } else {
     P.fd_fore = fdfore;
   }
@@ -618,6 +638,14 @@ int hxg_destroy(hxg_handle *h) {
     if (b.p) cudaFree(b.p);
   for (auto &b : h->out)
     if (b.p) cudaFree(b.p);
+  for (auto &b : h->ck)
+    if (b.p) cudaFree(b.p);
+  for (auto &b : h->ck_inner)
+    if (b.p) cudaFree(b.p);
+  for (auto *b : {&h->grad_rec, &h->grad_par, &h->g_fdmap})
+    if (b->p) cudaFree(b->p);
+  for (auto &b : h->g_shell)
+    if (b.p) cudaFree(b.p);
   for (auto &e : h->events) {
     cudaEventDestroy(e.first);
     cudaEventDestroy(e.second);
@@ -734,6 +762,19 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
     const int C = choose_chunks(h, npix, step);
     P.chunks = C;
     P.log2_chunks = hpx_ilog2((uint64_t)C);
+    if (h->checkpoint && !fp32) {
+      if (h->ck.size() < o->total_shell) {
+        h->ck.resize(o->total_shell);
+        h->ck_inner.resize(o->total_shell);
+        h->ck_chunks.resize(o->total_shell);
+      }
+      if ((st = ensure(h, h->ck[s], npix * C * 3 * sizeof(double))) != HXG_OK) return st;
+      if ((st = ensure(h, h->ck_inner[s], npix * sizeof(double))) != HXG_OK) return st;
+      HXG_CK(cudaMemsetAsync(h->ck_inner[s].p, 0, npix * sizeof(double), h->stream));
+      P.ck = static_cast<double *>(h->ck[s].p);
+      P.ck_inner = static_cast<double *>(h->ck_inner[s].p);
+      h->ck_chunks[s] = C;
+    }
     const uint64_t warps = (npix + (32 / C) - 1) / (32 / C);
     const unsigned threads = 256;
     const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
@@ -771,6 +812,132 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
       ++h->launch_count;
     }
   }
+  if (h->checkpoint && !fp32) {
+    h->ck_valid = true;
+    h->ck_obs = *o;
+    h->ck_models = h->models;
+  } else {
+    h->ck_valid = false;
+  }
+  return HXG_OK;
+}
+
+int hxg_set_checkpointing(hxg_handle *h, int enable) {
+  if (!h) return HXG_ERR_INVALID;
+  if (enable && h->precision != HXG_FP64)
+    return fail(h, HXG_ERR_UNSUPPORTED, "the adjoint runs on the FP64 form only");
+  h->checkpoint = enable != 0;
+  h->ck_valid = false;
+  return HXG_OK;
+}
+
+// Reverse-mode pass over the shells of the last checkpointed forward call
+// (integrator.cc:23-228 differentiated): outer shells first, so that the
+// inner-shell Faraday-depth gradients of shell s reach shells < s.
+int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
+                       const double *g_fd, const double *g_is,
+                       const double *g_qs, const double *g_us,
+                       double *d_grad_params, double *d_grad_bx,
+                       double *d_grad_by, double *d_grad_bz,
+                       double *d_grad_ne) {
+  if (!h || !o) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  if (!h->ck_valid || std::memcmp(&h->ck_obs, o, sizeof(*o)) != 0 ||
+      std::memcmp(&h->ck_models, &h->models, sizeof(h->models)) != 0)
+    return fail(h, HXG_ERR_STATE,
+                "no checkpointed forward pass for these obs/models (enable "
+                "hxg_set_checkpointing and call hxg_write_grid_device first)");
+  if (h->groups.size() > 1)
+    return fail(h, HXG_ERR_UNSUPPORTED, "the adjoint supports one grid geometry");
+  int st;
+  const size_t ngrid = h->groups.empty() ? 0 : h->groups[0].n;
+  if (ngrid) {
+    if ((st = ensure(h, h->grad_rec, ngrid * 4 * sizeof(double))) != HXG_OK) return st;
+    HXG_CK(cudaMemsetAsync(h->grad_rec.p, 0, ngrid * 4 * sizeof(double), h->stream));
+  }
+  if ((st = ensure(h, h->grad_par, kNumParams * sizeof(double))) != HXG_OK) return st;
+  HXG_CK(cudaMemsetAsync(h->grad_par.p, 0, kNumParams * sizeof(double), h->stream));
+  double *gfdmap = nullptr;
+  if (o->do_fd) {
+    const size_t b = npix_of(o->nside_fd) * sizeof(double);
+    if ((st = ensure(h, h->g_fdmap, b)) != HXG_OK) return st;
+    gfdmap = static_cast<double *>(h->g_fdmap.p);
+    if (g_fd)
+      HXG_CK(cudaMemcpyAsync(gfdmap, g_fd, b, cudaMemcpyDeviceToDevice, h->stream));
+    else
+      HXG_CK(cudaMemsetAsync(gfdmap, 0, b, h->stream));
+  }
+  uint32_t max_nside = 0;
+  for (uint32_t s = 0; s < o->total_shell; ++s) max_nside = std::max(max_nside, o->nside_shell[s]);
+  for (int k = 0; k < 5; ++k)
+    if ((st = ensure(h, h->g_shell[k], npix_of(max_nside) * sizeof(double))) != HXG_OK)
+      return st;
+  double *gs[5];
+  for (int k = 0; k < 5; ++k) gs[k] = static_cast<double *>(h->g_shell[k].p);
+  for (int s = (int)o->total_shell - 1; s >= 0; --s) {
+    ShellLaunch F;
+    uint64_t step;
+    if ((st = build_launch(h, *o, (uint32_t)s, F, step)) != HXG_OK) return st;
+    const int ns = (int)o->nside_shell[s];
+    const uint64_t npix = npix_of((uint32_t)ns);
+    for (int k = 0; k < 5; ++k)
+      HXG_CK(cudaMemsetAsync(gs[k], 0, npix * sizeof(double), h->stream));
+    // transposes of the shell merges (integrator.cc:121-132)
+    if (o->do_dm && g_dm)
+      HXG_CK(launch_accumulate_transpose(h->stream, (int)o->nside_dm, ns, g_dm, gs[0], 1.));
+    if (o->do_fd)
+      HXG_CK(launch_accumulate_transpose(h->stream, (int)o->nside_fd, ns, gfdmap, gs[1], 1.));
+    if (o->do_sync) {
+      const double tc = F.tc_a * F.tc_a / F.tc_b;
+      const double *gsy[3] = {g_is, g_qs, g_us};
+      for (int k = 0; k < 3; ++k)
+        if (gsy[k])
+          HXG_CK(launch_accumulate_transpose(h->stream, (int)o->nside_sync, ns, gsy[k],
+                                             gs[2 + k], tc));
+    }
+    F.fdmap = o->do_fd ? gfdmap : nullptr;  // non-null marks inner-FD use
+    F.nside_fdmap = o->do_fd ? (int)o->nside_fd : 0;
+    F.mask = nullptr;
+    if (o->do_mask) {
+      const unsigned char *dmk = nullptr;
+      if ((st = device_mask(h, o->nside_shell[s], &dmk)) != HXG_OK) return st;
+      F.mask = dmk;
+    }
+    const int C = h->ck_chunks[s];
+    F.chunks = C;
+    F.log2_chunks = hpx_ilog2((uint64_t)C);
+    AdjointLaunch A{};
+    A.F = F;
+    A.ck = static_cast<const double *>(h->ck[s].p);
+    A.ck_inner = static_cast<const double *>(h->ck_inner[s].p);
+    for (int k = 0; k < 5; ++k) A.g[k] = gs[k];
+    A.grad_rec = ngrid ? static_cast<double *>(h->grad_rec.p) : nullptr;
+    A.grad_par = static_cast<double *>(h->grad_par.p);
+    A.g_fdmap = gfdmap;
+    A.want_j0 = (h->models.cre == HXG_CRE_ANA || h->models.cre == HXG_CRE_UNIF) ? 1 : 0;
+    const uint64_t warps = (npix + (32 / C) - 1) / (32 / C);
+    const unsigned threads = 256;
+    const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
+    HXG_CK(launch_adjoint(h->stream, A, blocks, threads));
+    ++h->launch_count;
+  }
+  // parameter gradients: j0 slot holds sum (dL/dJ) J, divide by j0
+  double gp[kNumParams];
+  HXG_CK(cudaMemcpyAsync(gp, h->grad_par.p, sizeof(gp), cudaMemcpyDeviceToHost, h->stream));
+  HXG_CK(cudaStreamSynchronize(h->stream));
+  const double j0 = h->models.cre == HXG_CRE_ANA ? h->models.cre_ana.j0
+                                                 : h->models.cre_unif.j0;
+  gp[7] = (j0 != 0.) ? gp[7] / j0 : 0.;
+  if (d_grad_params)
+    HXG_CK(cudaMemcpyAsync(d_grad_params, gp, sizeof(gp), cudaMemcpyHostToDevice, h->stream));
+  if (ngrid && (d_grad_bx || d_grad_ne)) {
+    const Group &G = h->groups[0];
+    const bool has_b = G.b_slots[0] >= 0, has_t = G.t_slots[0] >= 0;
+    HXG_CK(launch_unpack_grad(h->stream, ngrid, static_cast<const double *>(h->grad_rec.p),
+                              has_b ? d_grad_bx : nullptr, has_b ? d_grad_by : nullptr,
+                              has_b ? d_grad_bz : nullptr, has_t ? d_grad_ne : nullptr));
+  }
+  HXG_CK(cudaStreamSynchronize(h->stream));
   return HXG_OK;
 }
 
@@ -1018,7 +1185,7 @@ int hxg_read_grid(hxg_handle *h, int field, uint64_t n, const double *pos,
   HXG_CK(cudaMemcpy(dpos, p.data(), 3 * n * 8, cudaMemcpyHostToDevice));
   HXG_CK(launch_read_group(0, fp32, D, n, dpos, dout));
   HXG_CK(cudaMemcpy(res.data(), dout, 4 * n * 8, cudaMemcpyDeviceToHost));
-  const double bu = fp32 ? cgs::muGauss : 1.0;
+  const double bu = fp32 ? cgs::fp32_bunit : 1.0;
   const bool vec = field == HXG_FIELD_BREG || field == HXG_FIELD_BRND;
   for (uint64_t i = 0; i < n; ++i) {
     if (vec)

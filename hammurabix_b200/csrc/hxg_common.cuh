@@ -27,6 +27,11 @@ constexpr double eV = (1.60217733e-12 * erg);
 constexpr double GeV = (1.e9 * eV);
 constexpr double GHz = 1.e9;
 constexpr double muGauss = 1.e-6;  // 1e-6 * sqrt(erg/cm^3)
+// Field unit of the FP32-compensated form (G).  A power of two, so that
+// rescaling FP32 grid voxels into it is exact: a rounded voxel would carry
+// the same error into every sample that reads it, which the Faraday phase
+// then amplifies.
+constexpr double fp32_bunit = 0x1p-20;
 constexpr double ccm = (cm * cm * cm);
 constexpr double c_light = (2.99792458e+10 * cm / sec);
 constexpr double h_planck = (6.626075540e-27 * erg * sec);

@@ -3,7 +3,7 @@
 //
 // Models are written once, templated on the working type T.  The FP64 form
 // evaluates them in CGS (the reference's own units and operation order);
-// the FP32 form evaluates them in kpc / muGauss / cm^-3 so that no
+// the FP32 form evaluates them in kpc / 2^-20 G / cm^-3 so that no
 // intermediate under- or overflows FP32.  All parameters arrive in a
 // DevModels block already converted to the form's working units.
 #pragma once

@@ -1,0 +1,351 @@
+// hxg_fp32c.cuh -- the FP32-compensated shell kernel.
+//
+// Precision split.  The Faraday depth n_e B_par is summed along the ray and
+// its running value sets every later sample's rotation 2 lambda^2 FD, which
+// reaches thousands of radians at 0.4 GHz.  A relative error rho in each
+// sample's n_e B_par therefore random-walks into a phase error of about
+// rho * phase / sqrt(samples); FP32 rounding of the analytic models (a few
+// ulp per sample) alone costs ~1e-5 in Q/U there.  So everything that feeds
+// n_e B_par is FP64 or exact:
+//   - the ray (observer, LOS versor, sample distance), the grid coordinates
+//     (cell index and fraction split exactly), the model cutoffs;
+//   - the analytic regular field and n_e (FP64; the spiral and exponential
+//     disk use an own exp and a Newton-refined rsqrt, and the spiral's B_par
+//     along the ray is amp/r * (K0 + K1 d) with per-ray K0, K1);
+//   - the product n_e B_par, the Faraday-depth and DM sums (FP64);
+//   - the phase, reduced to a fraction of a turn with integer operations.
+// FP32 carries the trilinear grid interpolation (FP32 voxel records, whose
+// rounding is random from sample to sample), the synchrotron emissivity and
+// polarisation angle, and Kahan-compensated I, Q, U sums.
+//
+// Speed.  The kernel is issue/latency bound (the grids stay in L1/L2) with
+// the XU pipe (MUFU and conversions) the busiest: the cell index and
+// fraction come from one FP64 add of a magic constant, the phase fraction
+// from integer operations, the |B_perp|^2 emissivity (CRE index 3) needs no
+// reciprocal, and the CRE profile uses two exponentials.
+#pragma once
+
+#include "hxg_integrate.cuh"
+
+// Resident blocks of 256 threads per SM the register allocation must allow.
+#ifndef HXG_FP32C_MIN_BLOCKS
+#define HXG_FP32C_MIN_BLOCKS 3
+#endif
+
+namespace hxg {
+
+// Cell index and fractional position along one axis from an FP64 grid
+// coordinate g with 0 < g < n-1 < 2^19.  Adding 1.5 * 2^20 leaves floor(g)
+// in the low 20 mantissa bits of the high word and frac(g) * 2^32, rounded,
+// in the low word; the fraction is rounded to 23 bits into [0, 1].
+__device__ __forceinline__ void cell_split(double g, int nmax2, int &cell,
+                                           float &frac) {
+  const double t = g + 1572864.0;
+  const unsigned lo = (unsigned)__double2loint(t);
+  const int hi = __double2hiint(t);
+  cell = (hi & 0xFFFFF) - 0x80000;
+  const unsigned long long r = ((unsigned long long)lo + 256ull) >> 9;
+  frac = __uint_as_float(0x3F800000u + (unsigned)r) - 1.0f;
+  if (cell > nmax2) {  // g within 2^-33 of n-1: stay in the last cell
+    cell = nmax2;
+    frac = 1.0f;
+  }
+}
+
+// Trilinear sample of one FP32 record group at the cell (x, y, z) with
+// fractions (fx, fy, fz): out[0..2] = B (2^-20 G), out[3] = n_e.
+__device__ __forceinline__ void trilinear_f32(const float4 *rec, int ny,
+                                              int nz, int x, int y, int z,
+                                              float fx, float fy, float fz,
+                                              float out[4]) {
+  const size_t nyz = (size_t)ny * (size_t)nz;
+  const size_t i00 = (size_t)x * nyz + (size_t)y * nz + z;
+  const size_t i01 = i00 + nz;
+  const size_t i10 = i00 + nyz;
+  const size_t i11 = i10 + nz;
+  const float4 c000 = __ldg(rec + i00), c001 = __ldg(rec + i00 + 1);
+  const float4 c010 = __ldg(rec + i01), c011 = __ldg(rec + i01 + 1);
+  const float4 c100 = __ldg(rec + i10), c101 = __ldg(rec + i10 + 1);
+  const float4 c110 = __ldg(rec + i11), c111 = __ldg(rec + i11 + 1);
+  const float gx = 1.f - fx, gy = 1.f - fy, gz = 1.f - fz;
+  const float a00 = gx * gy, a01 = gx * fy, a10 = fx * gy, a11 = fx * fy;
+  const float w000 = a00 * gz, w001 = a00 * fz, w010 = a01 * gz, w011 = a01 * fz;
+  const float w100 = a10 * gz, w101 = a10 * fz, w110 = a11 * gz, w111 = a11 * fz;
+#define HXG_TRI(c)                                                        \
+  fmaf(w111, c111.c, fmaf(w110, c110.c, fmaf(w101, c101.c, fmaf(w100, c100.c, \
+  fmaf(w011, c011.c, fmaf(w010, c010.c, fmaf(w001, c001.c, w000 * c000.c)))))))
+  out[0] = HXG_TRI(x);
+  out[1] = HXG_TRI(y);
+  out[2] = HXG_TRI(z);
+  out[3] = HXG_TRI(w);
+#undef HXG_TRI
+}
+
+// e^a for a < 700 (a below -700 is taken as -700).  Cody-Waite style
+// reduction a = k ln2 + f with k = nearest integer of a / ln2 (|f| <= ln2/2;
+// the rounding error of ln2 in FP64 times k stays below 1e-14), e^f from its
+// Taylor series to degree 10 (truncation below 3e-13 relative), 2^k added to
+// the exponent field.
+__device__ __forceinline__ double exp_fd(double a) {
+  const double kMagic = 6755399441055744.0;  // 1.5 * 2^52
+  a = fmax(a, -700.);
+  const double t = fma(a, 1.4426950408889634, kMagic);
+  const int k = __double2loint(t);
+  const double kd = t - kMagic;
+  const double f = fma(-kd, 0.6931471805599453, a);
+  double p = 2.755731922398589e-07;            // 1/10!
+  p = fma(p, f, 2.7557319223985893e-06);       // 1/9!
+  p = fma(p, f, 2.48015873015873e-05);         // 1/8!
+  p = fma(p, f, 0.0001984126984126984);        // 1/7!
+  p = fma(p, f, 0.001388888888888889);         // 1/6!
+  p = fma(p, f, 0.008333333333333333);         // 1/5!
+  p = fma(p, f, 0.041666666666666664);         // 1/4!
+  p = fma(p, f, 0.16666666666666666);          // 1/3!
+  p = fma(p, f, 0.5);
+  p = fma(p, f, 1.0);
+  p = fma(p, f, 1.0);
+  return __hiloint2double(__double2hiint(p) + (k << 20), __double2loint(p));
+}
+
+// 1/sqrt(t) for t > 0: the FP64 hardware estimate refined by two Newton
+// steps (relative error ~1e-15).
+__device__ __forceinline__ double rsqrt_fd(double t) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(t));
+  double e = fma(-t * y, y, 1.0);
+  y = fma(0.5 * y, e, y);
+  e = fma(-t * y, y, 1.0);
+  return fma(0.5 * y, e, y);
+}
+
+template <int NG>
+__global__ void __launch_bounds__(256, HXG_FP32C_MIN_BLOCKS)
+shell_fp32c_kernel(const ShellLaunch P) {
+  const int lane = threadIdx.x & 31;
+  const long long gw =
+      ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int C = P.chunks;
+  const int seg = lane >> P.log2_chunks;
+  const int c = lane & (C - 1);
+  const Hpx h = hpx_make((uint64_t)P.nside);
+  const unsigned long long nest =
+      (unsigned long long)gw * (32 >> P.log2_chunks) + seg;
+  const bool valid = nest < h.npix;
+  uint64_t ring = 0;
+  bool live = false;
+  if (valid) {
+    ring = hpx_nest2ring(h, nest);
+    live = (P.mask == nullptr) || (P.mask[ring] != 0);
+  }
+  double dm = 0., fd = 0., si = 0., sq = 0., su = 0.;
+  if (live) {
+    double th, ph;
+    hpx_pix2ang(h, ring, th, ph);
+    double inner = 0.;
+    if (P.fdmap != nullptr) {
+      const Hpx hf = hpx_make((uint64_t)P.nside_fdmap);
+      inner = hpx_interpolate(hf, P.fdmap, th, ph);
+    }
+    const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
+    const double ux = cp * st, uy = sp * st, uz = ct;
+    // LOS versor split into FP32 high + low parts for the grid projection
+    const float uxh = float(ux), uyh = float(uy), uzh = float(uz);
+    const float uxl = float(ux - double(uxh)), uyl = float(uy - double(uyh)),
+                uzl = float(uz - double(uzh));
+    const float etx = float(ct * cp), ety = float(ct * sp), etz = float(-st);
+    const float epx = float(-sp), epy = float(cp);
+    const double ox = P.obs[0], oy = P.obs[1], oz = P.obs[2];
+    // |pos|^2 along the ray: |o|^2 + 2 (o.u) d + d^2
+    const double ou2 = 2. * (ox * ux + oy * uy + oz * uz);
+    const double oo = ox * ox + oy * oy + oz * oz;
+    const double r2min = P.gc_r_min * P.gc_r_min, r2max = P.gc_r_max * P.gc_r_max;
+    // Faraday phase in turns: rev0 + rev_k * (FD sum)
+    const double rev0 = P.lambda2 * inner * (1. / cgs::pi);
+    const double rev_k = P.phase_k * (0.5 / cgs::pi);
+    const DevModels &M = P.models;
+    const FastModels &F = P.fast;
+    const float pe = float(P.em_pe);
+    const bool pe2 = P.em_const && P.em_pe == 2.;
+    const float a_s = float(P.a_s);
+    const float cre_ir0 = float(1. / M.cre_r0), cre_2iz0 = float(2. / M.cre_z0);
+    const float cre_R0 = float(M.cre_R0);
+    // grid-space ray of group 0: g(d) = g0 + gv d
+    double g0x = 0., g0y = 0., g0z = 0., gvx = 0., gvy = 0., gvz = 0.;
+    if (NG == 1) {
+      const DevGridGroup &G = P.groups[0];
+      g0x = (ox - G.lo[0]) * G.scale[0];
+      g0y = (oy - G.lo[1]) * G.scale[1];
+      g0z = (oz - G.lo[2]) * G.scale[2];
+      gvx = ux * G.scale[0];
+      gvy = uy * G.scale[1];
+      gvz = uz * G.scale[2];
+    }
+    // spiral B_par along the ray: amp/r * (K0 + K1 d)
+    const double K0 = F.sp_sin * (ox * ux + oy * uy) + F.sp_cos * (ox * uy - oy * ux);
+    const double K1 = F.sp_sin * (ux * ux + uy * uy);
+    const float spf = float(F.sp_sin), cpf = float(F.sp_cos);
+    KahanF ki{0.f, 0.f}, kq{0.f, 0.f}, ku{0.f, 0.f};
+    double sfd = 0., sdm = 0.;
+    const bool fast_b = M.breg == kBregSpiral;
+    const bool slow_b = M.breg != kBregNone && M.breg != kBregGrid && !fast_b;
+    const bool fast_t = M.tereg == kTeregExpdisk;
+    const bool slow_t = M.tereg != kTeregNone && M.tereg != kTeregGrid && !fast_t;
+    const double rc2_hi = 400. * M.kpc * M.kpc, rc2_lo = 9. * M.kpc * M.kpc;
+    float last_index = __int_as_float(0x7fc00000), gt = float(P.em_gt),
+          gp = float(P.em_gp), inv1mi = 1.f;
+    const long long i0 = (P.step * c) >> P.log2_chunks;
+    const long long i1 = (P.step * (c + 1)) >> P.log2_chunks;
+    double d = P.d_start + ((double)i0 + 0.5) * P.delta;
+    for (long long i = i0; i < i1; ++i, d += P.delta) {
+      const double pz = fma(uz, d, oz);
+      const double r2 = fma(d, d + ou2, oo);
+      if (r2 < r2min || r2 > r2max || pz < P.gc_z_min || pz > P.gc_z_max) continue;
+      const double px = fma(ux, d, ox);
+      const double py = fma(uy, d, oy);
+      const double p3[3] = {px, py, pz};
+      const float xf = float(px), yf = float(py), zf = float(pz);
+      // FP64 analytic part of B_par and n_e; FP32 field for the synchrotron
+      double bp_d = 0., te_d = 0.;
+      float bxr = 0.f, byr = 0.f, bzr = 0.f;
+      if (fast_b || fast_t) {
+        const double rc2 = fma(px, px, py * py);
+        const double y = rsqrt_fd(rc2);
+        const double r = rc2 > 0. ? rc2 * y : 0.;
+        if (fast_b && !(rc2 > rc2_hi || rc2 < rc2_lo)) {
+          const double ay =
+              F.sp_b0 * exp_fd(fma(-r, F.sp_irs, fma(-fabs(pz), F.sp_ihs, F.sp_crs))) * y;
+          bp_d = ay * fma(K1, d, K0);
+          const float ayf = float(ay);
+          bxr = ayf * (spf * xf - cpf * yf);
+          byr = ayf * (spf * yf + cpf * xf);
+        }
+        if (fast_t) te_d = F.ex_n0 * exp_fd(-fma(r, F.ex_irn, fabs(pz) * F.ex_ihn));
+      }
+      if (slow_b) {
+        const V3<double> Br = breg_model<double>(M, px, py, pz, p3);
+        bp_d = fma(Br.x, ux, fma(Br.y, uy, Br.z * uz));
+        bxr = float(Br.x);
+        byr = float(Br.y);
+        bzr = float(Br.z);
+      }
+      if (slow_t) te_d = tereg_model<double>(M, px, py, pz, p3);
+      float bg[4] = {0.f, 0.f, 0.f, 0.f};
+      if (NG == 1) {
+        const DevGridGroup &G = P.groups[0];
+        const double gx = fma(gvx, d, g0x), gy = fma(gvy, d, g0y), gz = fma(gvz, d, g0z);
+        if (gx > 0. && gx < double(G.nx - 1) && gy > 0. && gy < double(G.ny - 1) &&
+            gz > 0. && gz < double(G.nz - 1)) {
+          int cx, cy, cz;
+          float fx, fy, fz;
+          cell_split(gx, G.nx - 2, cx, fx);
+          cell_split(gy, G.ny - 2, cy, fy);
+          cell_split(gz, G.nz - 2, cz, fz);
+          trilinear_f32(reinterpret_cast<const float4 *>(G.rec), G.ny, G.nz, cx, cy, cz,
+                        fx, fy, fz, bg);
+        }
+      } else if (NG > 1) {
+        float b3[3] = {0.f, 0.f, 0.f};
+        CellCache<float> cc;
+#pragma unroll 1
+        for (int g = 0; g < P.ngroups; ++g) {
+          cc.key = -1;
+          sample_group<float, false>(P.groups[g], px, py, pz, cc, b3, bg[3]);
+        }
+        bg[0] = b3[0];
+        bg[1] = b3[1];
+        bg[2] = b3[2];
+      }
+      // n_e (clamped at 0, integrator.cc:201) and n_e B_par in FP64
+      double te = te_d + double(bg[3]);
+      te = te > 0. ? te : 0.;
+      const float bpg = fmaf(bg[0], uxh, fmaf(bg[1], uyh, bg[2] * uzh)) +
+                        fmaf(bg[0], uxl, fmaf(bg[1], uyl, bg[2] * uzl));
+      sdm += te;
+      sfd = fma(te, bp_d + double(bpg), sfd);
+      if (P.do_sync) {
+        const float bx = bxr + bg[0], by = byr + bg[1], bz = bzr + bg[2];
+        // B_perp on the sky basis: |B_perp|^2 = xv^2 + yv^2, and the IAU
+        // angle has cos 2ipa = (xv^2 - yv^2) / |B_perp|^2 and
+        // sin 2ipa = 2 xv yv / |B_perp|^2 (integrator.cc:257-265)
+        const float xv = -(epx * bx + epy * by);
+        const float yv = -(etx * bx + ety * by + etz * bz);
+        const float rr = fmaf(xv, xv, yv * yv);
+        const float cc2 = fmaf(xv, xv, -yv * yv), ss2 = 2.f * xv * yv;
+        float prof;
+        if (M.cre == kCreAna) {
+          // exp((R0 - r)/r0) sech^2(z/z0)
+          //   = 4 exp((R0 - r)/r0 - 2|z|/z0) / (1 + exp(-2|z|/z0))^2
+          const float r2f = fmaf(xf, xf, yf * yf);
+          const float rf = r2f * rsqrtf(fmaxf(r2f, 1e-30f));
+          const float az2 = fabsf(zf) * cre_2iz0;
+          const float t = __expf(-az2);
+          const float den = 1.f + t;
+          prof = __fdividef(4.f * __expf((cre_R0 - rf) * cre_ir0 - az2), den * den);
+        } else {
+          prof = cre_profile<float>(M, xf, yf, zf, p3);
+        }
+        float wt, wpc, wps;
+        if (pe2) {
+          wt = prof * rr;
+          wpc = prof * cc2;
+          wps = prof * ss2;
+        } else {
+          float wp;
+          if (P.em_const) {
+            const float bp = (pe == 1.f) ? sqrtf(rr) : powf(rr, 0.5f * pe);
+            wt = wp = prof * bp;
+          } else {
+            const float index = cre_index<float>(M, xf, yf, zf);
+            if (index != last_index) {
+              gt = tgammaf(-0.25f * index + 19.f / 12.f) * tgammaf(-0.25f * index - 1.f / 12.f);
+              gp = tgammaf(-0.25f * index + 7.f / 12.f) * tgammaf(-0.25f * index - 1.f / 12.f);
+              inv1mi = 1.f / (1.f - index);
+              last_index = index;
+            }
+            const float bper = sqrtf(rr);
+            const float Ae = exp2f(0.5f * (index + 1.f) * log2f(a_s / bper));
+            const float base = prof * bper * Ae;
+            wt = base * gt * inv1mi;
+            wp = base * gp;
+          }
+          // ipa of a zero B_perp is 0 (atan2(0, 0)): cos 2ipa = 1
+          const float inv = rr > 0.f ? __frcp_rn(rr) : 0.f;
+          wpc = rr > 0.f ? wp * cc2 * inv : wp;
+          wps = wp * ss2 * inv;
+        }
+        ki.add(wt);
+        // Faraday phase: the turn count rev0 + rev_k * FD in FP64, its
+        // fraction rounded to 2^-23 turn in [-1/2, 1/2) with integer ops
+        const double rev = fma(rev_k, sfd, rev0) + 1572864.0;
+        const int q = (int)((unsigned)__double2loint(rev) + 256u) >> 9;
+        const float ang =
+            (__int_as_float(0x4B400000 + q) - 12582912.0f) * 7.490140565847857e-07f;
+        float sf, cf;
+        __sincosf(ang, &sf, &cf);
+        kq.add(fmaf(wpc, cf, -wps * sf));
+        ku.add(fmaf(wpc, sf, wps * cf));
+      }
+    }
+    dm = sdm * P.k_dm;
+    fd = sfd * P.fd_fore;
+    si = ki.value() * P.k_t;
+    sq = kq.value() * P.k_p;
+    su = ku.value() * P.k_p;
+  }
+  combine_chunks(P, c, 2. * P.lambda2, dm, fd, si, sq, su);
+  if (live && c == 0) {
+    if (P.do_dm) P.out[0][ring] = dm;
+    if (P.do_fd || P.do_sync) P.out[1][ring] = fd;
+    if (P.do_sync) {
+      P.out[2][ring] = si * P.tc_a * P.tc_a / P.tc_b;
+      P.out[3][ring] = sq * P.tc_a * P.tc_a / P.tc_b;
+      P.out[4][ring] = su * P.tc_a * P.tc_a / P.tc_b;
+    }
+  } else if (valid && !live && c == 0) {
+    if (P.do_dm) P.out[0][ring] = 0.;
+    if (P.do_fd || P.do_sync) P.out[1][ring] = 0.;
+    if (P.do_sync) P.out[2][ring] = P.out[3][ring] = P.out[4][ring] = 0.;
+  }
+}
+
+}  // namespace hxg

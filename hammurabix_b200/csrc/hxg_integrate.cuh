@@ -19,6 +19,14 @@ namespace hxg {
 
 constexpr int kMaxGroups = 4;
 
+// FP32C evaluation of the spiral B and exponential n_e models (FP64, kpc
+// and 2^-20 G, reciprocals precomputed).
+struct FastModels {
+  double sp_b0, sp_irs, sp_crs, sp_ihs;  // amplitude, 1/r_s, r_sun/r_s, 1/h_s
+  double sp_sin, sp_cos;                 // sin, cos of the pitch angle
+  double ex_n0, ex_irn, ex_ihn;          // exp-disk n0, 1/r_s, 1/h_s
+};
+
 // Everything one shell launch needs, in the working units of its form.
 struct ShellLaunch {
   double obs[3];             // observer
@@ -32,7 +40,7 @@ struct ShellLaunch {
   const unsigned char *mask; // 1 = integrate (integrator.cc:69-70), or null
   double *out[5];            // shell maps (RING): dm, fd, is, qs, us
   // FD and synchrotron constants
-  double fd_fore;            // FP64: -qe^3/(2 pi mec2^2); FP32C: that * delta * muG
+  double fd_fore;            // FP64: -qe^3/(2 pi mec2^2); FP32C: that * delta * 2^-20 G
   double lambda2;            // (c/nu)^2
   double i2bt;               // c^2 / (2 kB nu^2)
   double tc_a, tc_b;         // temp_convert(t) = t*a*a/b (integrator.cc:275-279)
@@ -46,11 +54,16 @@ struct ShellLaunch {
   // FP32C scales (applied in FP64 after the sums)
   double k_t, k_p, k_dm;     // I, Q/U and DM scale factors
   double phase_k;            // 2 lambda^2 * fd_fore (per FP64 FD-sum unit)
-  double a_s;                // A * |B_perp| in muG (variable-index path)
+  double a_s;                // A * |B_perp| in 2^-20 G (variable-index path)
   double em_pe;              // exponent of |B_perp| (constant index, FP32C)
   DevModels models;
   DevGridGroup groups[kMaxGroups];
   int ngroups;
+  // adjoint checkpoint (FP64 form): per (pixel, chunk) the chunk's FD, Q, U
+  // before the chunk combination, per pixel the inner-shell FD; null = off
+  double *ck;
+  double *ck_inner;
+  FastModels fast;  // FP32C only
 };
 
 // Kahan-compensated FP32 accumulator.
@@ -153,6 +166,7 @@ shell_fp64_kernel(const ShellLaunch P) {
       const Hpx hf = hpx_make((uint64_t)P.nside_fdmap);
       inner = hpx_interpolate(hf, P.fdmap, th, ph);
     }
+    if (P.ck_inner != nullptr && c == 0) P.ck_inner[ring] = inner;
     const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
     // los_versor (integrator.cc:268-272)
     const double ux = cp * st, uy = sp * st, uz = ct;
@@ -231,6 +245,12 @@ shell_fp64_kernel(const ShellLaunch P) {
       }
     }
   }
+  if (P.ck != nullptr && live) {
+    const unsigned long long ci = nest * (unsigned long long)C + c;
+    P.ck[3 * ci] = fd;
+    P.ck[3 * ci + 1] = sq;
+    P.ck[3 * ci + 2] = su;
+  }
   combine_chunks(P, c, rot_k, dm, fd, si, sq, su);
   if (live && c == 0) {
     if (P.do_dm) P.out[0][ring] = dm;
@@ -242,146 +262,6 @@ shell_fp64_kernel(const ShellLaunch P) {
     }
   } else if (valid && !live && c == 0) {
     // masked pixel: every observable is zero (integrator.cc:63-67, 98-115)
-    if (P.do_dm) P.out[0][ring] = 0.;
-    if (P.do_fd || P.do_sync) P.out[1][ring] = 0.;
-    if (P.do_sync) P.out[2][ring] = P.out[3][ring] = P.out[4][ring] = 0.;
-  }
-}
-
-// ===================================================================
-// FP32-compensated form
-// ===================================================================
-template <int NG, bool kCache>
-__global__ void __launch_bounds__(256)
-shell_fp32c_kernel(const ShellLaunch P) {
-  const int lane = threadIdx.x & 31;
-  const long long gw =
-      ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int C = P.chunks;
-  const int seg = lane >> P.log2_chunks;
-  const int c = lane & (C - 1);
-  const Hpx h = hpx_make((uint64_t)P.nside);
-  const unsigned long long nest =
-      (unsigned long long)gw * (32 >> P.log2_chunks) + seg;
-  const bool valid = nest < h.npix;
-  uint64_t ring = 0;
-  bool live = false;
-  if (valid) {
-    ring = hpx_nest2ring(h, nest);
-    live = (P.mask == nullptr) || (P.mask[ring] != 0);
-  }
-  double dm = 0., fd = 0., si = 0., sq = 0., su = 0.;
-  if (live) {
-    // FP64: pointing, LOS versor and inner-shell Faraday depth
-    double th, ph;
-    hpx_pix2ang(h, ring, th, ph);
-    double inner = 0.;
-    if (P.fdmap != nullptr) {
-      const Hpx hf = hpx_make((uint64_t)P.nside_fdmap);
-      inner = hpx_interpolate(hf, P.fdmap, th, ph);
-    }
-    const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
-    const double ux = cp * st, uy = sp * st, uz = ct;
-    const float uxf = float(ux), uyf = float(uy), uzf = float(uz);
-    const float etx = float(ct * cp), ety = float(ct * sp), etz = float(-st);
-    const float epx = float(-sp), epy = float(cp);
-    const double r2min = P.gc_r_min * P.gc_r_min, r2max = P.gc_r_max * P.gc_r_max;
-    const double phi0 = 2. * P.lambda2 * inner;
-    const DevModels &M = P.models;
-    const float pe = float(P.em_pe);
-    const float a_s = float(P.a_s);
-    CellCache<float> cache;
-    cache.key = -1;
-    KahanF kdm{0.f, 0.f}, ki{0.f, 0.f}, kq{0.f, 0.f}, ku{0.f, 0.f};
-    double sfd = 0.;
-    float last_index = __int_as_float(0x7fc00000), gt = float(P.em_gt),
-          gp = float(P.em_gp), inv1mi = 1.f;
-    const long long i0 = (P.step * c) >> P.log2_chunks;
-    const long long i1 = (P.step * (c + 1)) >> P.log2_chunks;
-    for (long long i = i0; i < i1; ++i) {
-      const double d = P.d_start + ((double)i + 0.5) * P.delta;
-      const double px = fma(ux, d, P.obs[0]);
-      const double py = fma(uy, d, P.obs[1]);
-      const double pz = fma(uz, d, P.obs[2]);
-      const double r2 = fma(px, px, fma(py, py, pz * pz));
-      if (r2 < r2min || r2 > r2max || pz < P.gc_z_min || pz > P.gc_z_max)
-        continue;
-      const float x = float(px), y = float(py), z = float(pz);
-      const double p3[3] = {px, py, pz};
-      V3<float> B = breg_model<float>(M, x, y, z, p3);
-      float te = tereg_model<float>(M, x, y, z, p3);
-      if (NG > 0) {
-        float b3[3] = {B.x, B.y, B.z};
-#pragma unroll 1
-        for (int g = 0; g < (NG == 1 ? 1 : P.ngroups); ++g)
-          sample_group<float, kCache>(P.groups[g], px, py, pz, cache, b3, te);
-        B.x = b3[0];
-        B.y = b3[1];
-        B.z = b3[2];
-      }
-      te = te > 0.f ? te : 0.f;
-      const float bpar = B.x * uxf + B.y * uyf + B.z * uzf;
-      const float cx = B.y * uzf - B.z * uyf;
-      const float cy = B.z * uxf - B.x * uzf;
-      const float cz = B.x * uyf - B.y * uxf;
-      const float bper = sqrtf(cx * cx + cy * cy + cz * cz);
-      if (P.do_dm) kdm.add(te);
-      if (P.do_fd || P.do_sync) sfd += double(te * bpar);
-      if (P.do_sync) {
-        const float prof = cre_profile<float>(M, x, y, z, p3);
-        float wt, wp;
-        if (P.em_const) {
-          float bp;
-          if (pe == 2.f)
-            bp = bper * bper;
-          else if (pe == 1.f)
-            bp = bper;
-          else
-            bp = powf(bper, pe);
-          wt = wp = prof * bp;
-        } else {
-          const float index = cre_index<float>(M, x, y, z);
-          if (index != last_index) {
-            gt = tgammaf(-0.25f * index + 19.f / 12.f) * tgammaf(-0.25f * index - 1.f / 12.f);
-            gp = tgammaf(-0.25f * index + 7.f / 12.f) * tgammaf(-0.25f * index - 1.f / 12.f);
-            inv1mi = 1.f / (1.f - index);
-            last_index = index;
-          }
-          const float Ae = exp2f(0.5f * (index + 1.f) * log2f(a_s / bper));
-          const float base = prof * bper * Ae;
-          wt = base * gt * inv1mi;
-          wp = base * gp;
-        }
-        ki.add(wt);
-        float c2, s2;
-        ipa2<float>(-(epx * B.x + epy * B.y), -(etx * B.x + ety * B.y + etz * B.z),
-                    c2, s2);
-        // FP64 Faraday phase, reduced to [-pi, pi] before FP32 sincos
-        const double phi = fma(P.phase_k, sfd, phi0);
-        const double kk = rint(phi * (1. / cgs::twopi));
-        const float rph = float(fma(-kk, cgs::twopi, phi));
-        float sf, cf;
-        sincosf(rph, &sf, &cf);
-        kq.add(wp * (cf * c2 - sf * s2));
-        ku.add(wp * (sf * c2 + cf * s2));
-      }
-    }
-    dm = kdm.value() * P.k_dm;
-    fd = sfd * P.fd_fore;
-    si = ki.value() * P.k_t;
-    sq = kq.value() * P.k_p;
-    su = ku.value() * P.k_p;
-  }
-  combine_chunks(P, c, 2. * P.lambda2, dm, fd, si, sq, su);
-  if (live && c == 0) {
-    if (P.do_dm) P.out[0][ring] = dm;
-    if (P.do_fd || P.do_sync) P.out[1][ring] = fd;
-    if (P.do_sync) {
-      P.out[2][ring] = si * P.tc_a * P.tc_a / P.tc_b;
-      P.out[3][ring] = sq * P.tc_a * P.tc_a / P.tc_b;
-      P.out[4][ring] = su * P.tc_a * P.tc_a / P.tc_b;
-    }
-  } else if (valid && !live && c == 0) {
     if (P.do_dm) P.out[0][ring] = 0.;
     if (P.do_fd || P.do_sync) P.out[1][ring] = 0.;
     if (P.do_sync) P.out[2][ring] = P.out[3][ring] = P.out[4][ring] = 0.;

@@ -10,6 +10,7 @@ namespace hxg {
 
 struct ShellLaunch;
 struct DevGridGroup;
+struct AdjointLaunch;
 
 cudaError_t launch_accumulate(cudaStream_t s, int nside_dst, int nside_src,
                               int nmaps, double *const *dst,
@@ -32,5 +33,13 @@ cudaError_t launch_pack(cudaStream_t s, bool fp32, uint64_t n, void *rec,
                         double tscale);
 cudaError_t launch_shell(cudaStream_t s, bool fp32, const ShellLaunch &P,
                          unsigned blocks, unsigned threads);
+cudaError_t launch_accumulate_transpose(cudaStream_t s, int nside_out,
+                                        int nside_shell, const double *g_out,
+                                        double *g_shell, double scale);
+cudaError_t launch_adjoint(cudaStream_t s, const AdjointLaunch &A,
+                           unsigned blocks, unsigned threads);
+cudaError_t launch_unpack_grad(cudaStream_t s, uint64_t n, const double *rec,
+                               double *gbx, double *gby, double *gbz,
+                               double *gne);
 
 }  // namespace hxg

@@ -2,6 +2,8 @@
 // packing, and the instantiations of the shell-integration kernels.
 #include <cuda_runtime.h>
 
+#include "hxg_adjoint.cuh"
+#include "hxg_fp32c.cuh"
 #include "hxg_integrate.cuh"
 #include "hxg_internal.h"
 
@@ -126,6 +128,44 @@ __global__ void pack_kernel(uint64_t n, T *rec, const double *bx0,
   rec[4 * i + 3] = T(te * tscale);
 }
 
+// dL/d(shell map) from dL/d(output map): the transpose of Hampix::accumulate
+// (include/hamdis.h:698-721).  Same Nside: g_shell += scale * g_out; else
+// each output pixel scatters its gradient to the 4 interpolation pixels.
+__global__ void accumulate_transpose_kernel(int nside_out, int nside_shell,
+                                            const double *g_out,
+                                            double *g_shell, double scale) {
+  const Hpx ho = hpx_make((uint64_t)nside_out);
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ho.npix) return;
+  const double g = g_out[i] * scale;
+  if (g == 0.) return;
+  if (nside_out == nside_shell) {
+    g_shell[i] += g;
+    return;
+  }
+  const Hpx hs = hpx_make((uint64_t)nside_shell);
+  double th, ph;
+  hpx_pix2ang(ho, i, th, ph);
+  uint64_t pix[4];
+  double w[4];
+  hpx_interp_weights(hs, th, ph, pix, w);
+  const double wtot = w[0] + w[1] + w[2] + w[3];
+  for (int k = 0; k < 4; ++k) atomicAdd(g_shell + pix[k], g * w[k] / wtot);
+}
+
+// Split the group-record gradient [N][4] into B (3 SoA arrays) and n_e.
+__global__ void unpack_grad_kernel(uint64_t n, const double *rec, double *gbx,
+                                   double *gby, double *gbz, double *gne) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (gbx) {
+    gbx[i] = rec[4 * i];
+    gby[i] = rec[4 * i + 1];
+    gbz[i] = rec[4 * i + 2];
+  }
+  if (gne) gne[i] = rec[4 * i + 3];
+}
+
 // ---- launch wrappers -----------------------------------------------------
 static inline unsigned blocks_for(uint64_t n, unsigned tpb) {
   return (unsigned)((n + tpb - 1) / tpb);
@@ -195,19 +235,44 @@ cudaError_t launch_shell(cudaStream_t s, bool fp32, const ShellLaunch &P,
   const int ng = P.ngroups;
   if (fp32) {
     if (ng == 0)
-      shell_fp32c_kernel<0, false><<<blocks, threads, 0, s>>>(P);
+      shell_fp32c_kernel<0><<<blocks, threads, 0, s>>>(P);
     else if (ng == 1)
-      shell_fp32c_kernel<1, true><<<blocks, threads, 0, s>>>(P);
+      shell_fp32c_kernel<1><<<blocks, threads, 0, s>>>(P);
     else
-      shell_fp32c_kernel<4, false><<<blocks, threads, 0, s>>>(P);
+      shell_fp32c_kernel<4><<<blocks, threads, 0, s>>>(P);
   } else {
     if (ng == 0)
       shell_fp64_kernel<0, false><<<blocks, threads, 0, s>>>(P);
     else if (ng == 1)
-      shell_fp64_kernel<1, true><<<blocks, threads, 0, s>>>(P);
+      shell_fp64_kernel<1, false><<<blocks, threads, 0, s>>>(P);
     else
       shell_fp64_kernel<4, false><<<blocks, threads, 0, s>>>(P);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_accumulate_transpose(cudaStream_t s, int nside_out,
+                                        int nside_shell, const double *g_out,
+                                        double *g_shell, double scale) {
+  const uint64_t n = 12ull * nside_out * nside_out;
+  accumulate_transpose_kernel<<<blocks_for(n, 256), 256, 0, s>>>(
+      nside_out, nside_shell, g_out, g_shell, scale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint(cudaStream_t s, const AdjointLaunch &A,
+                           unsigned blocks, unsigned threads) {
+  if (A.F.ngroups == 0)
+    shell_fp64_adjoint_kernel<0><<<blocks, threads, 0, s>>>(A);
+  else
+    shell_fp64_adjoint_kernel<1><<<blocks, threads, 0, s>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_grad(cudaStream_t s, uint64_t n, const double *rec,
+                               double *gbx, double *gby, double *gbz,
+                               double *gne) {
+  unpack_grad_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, rec, gbx, gby, gbz, gne);
   return cudaGetLastError();
 }
 

@@ -97,6 +97,22 @@ class Integrator:
     def sync(self):
         _lib.check(self._lib.hxg_sync(self._h), self._h)
 
+    # ---- adjoint -----------------------------------------------------------
+    def set_checkpointing(self, enable=True):
+        """Store per-shell checkpoints in write_grid_device for adjoint()."""
+        _lib.check(self._lib.hxg_set_checkpointing(self._h, int(bool(enable))), self._h)
+
+    def adjoint_device(self, obs, g_dm=None, g_fd=None, g_is=None, g_qs=None, g_us=None,
+                       grad_params=None, grad_b=None, grad_ne=None):
+        """dL/d(maps) (torch CUDA float64) -> fills grad_params
+        (HXG_NUM_PARAMS), grad_b (3 tensors, one per B component) and
+        grad_ne (one tensor) with dL/d(parameters) and dL/d(grid values)."""
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        gb = list(grad_b) if grad_b is not None else [None, None, None]
+        _lib.check(self._lib.hxg_adjoint_device(
+            self._h, C.byref(obs), ptr(g_dm), ptr(g_fd), ptr(g_is), ptr(g_qs), ptr(g_us),
+            ptr(grad_params), ptr(gb[0]), ptr(gb[1]), ptr(gb[2]), ptr(grad_ne)), self._h)
+
     # ---- timing ----------------------------------------------------------
     def set_timing(self, enable=True):
         _lib.check(self._lib.hxg_set_timing(self._h, int(bool(enable))), self._h)

@@ -246,6 +246,39 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *obs, double *d_dm,
 /* Wait for the handle's stream; returns the first asynchronous error.     */
 int hxg_sync(hxg_handle *h);
 
+/* ---- adjoint (gradients of a scalar loss of the maps) -------------------
+ * Reverse mode of hxg_write_grid_device (FP64 form).  With checkpointing
+ * on, every forward call stores per shell the chunk Faraday depths and
+ * Q, U partial sums and the inner-shell Faraday depth of each pixel; the
+ * adjoint then runs one backward sweep per shell, outer shells first.
+ *
+ * Inputs: dL/d(output maps) on the device (same sizes as the forward's
+ * outputs; NULL = zero).  Outputs (device, overwritten, NULL = skip):
+ *   d_grad_params[HXG_NUM_PARAMS]: dL/d(parameter) in the order below, for
+ *     the spiral B model, the exponential n_e disk and the CRE j0 (zero for
+ *     the parameters of models that are not active);
+ *   d_grad_bx/by/bz: dL/d(B grid value) per voxel of the gridded B slot(s);
+ *   d_grad_ne: dL/d(n_e grid value) per voxel of the gridded n_e slot(s).
+ * One grid geometry at most.                                              */
+enum {
+  HXG_PARAM_SPIRAL_B0 = 0,
+  HXG_PARAM_SPIRAL_PITCH = 1,
+  HXG_PARAM_SPIRAL_R = 2,
+  HXG_PARAM_SPIRAL_H = 3,
+  HXG_PARAM_EXPDISK_N0 = 4,
+  HXG_PARAM_EXPDISK_R = 5,
+  HXG_PARAM_EXPDISK_H = 6,
+  HXG_PARAM_CRE_J0 = 7,
+  HXG_NUM_PARAMS = 8
+};
+int hxg_set_checkpointing(hxg_handle *h, int enable);
+int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *obs,
+                       const double *g_dm, const double *g_fd,
+                       const double *g_is, const double *g_qs,
+                       const double *g_us, double *d_grad_params,
+                       double *d_grad_bx, double *d_grad_by,
+                       double *d_grad_bz, double *d_grad_ne);
+
 /* ---- timing of the integration kernels ------------------------------
  * enable != 0: every shell-integration launch is bracketed by CUDA events
  * on the launching stream.  hxg_get_timing returns the summed device time

@@ -1,0 +1,127 @@
+"""Adjoint (hxg_adjoint_device through torch.autograd) against central finite
+differences of the FP64 forward, on a reduced config-4 workload: analytic
+spiral B + exponential n_e disk + CRE_ana, a random B grid (Grid_brnd) and a
+random n_e grid (Grid_ternd), three shells, DM + FD + sync with inner-shell
+Faraday rotation.
+
+Loss: sum over I, Q, U, FD, DM of w_k (map_k - target_k)^2 / sigma_k^2 with
+targets from 1%-perturbed parameters.  Finite differences: central
+differences with steps h and h/2 combined by Richardson extrapolation (error
+O(h^4): at 0.408 GHz the Faraday phase makes the loss strongly nonlinear),
+h = 1e-4 relative for parameters and 1e-4 of the grid rms for voxels.
+"""
+import numpy as np
+import pytest
+
+from hammurabix_b200 import abi, units as U, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _setup(freq_ghz):
+    from hammurabix_b200.autograd import LOSMaps, params_of
+    n = 16
+    obs = W.make_obs([4, 8, 16], 24.0, 0.1, freq_ghz=freq_ghz)
+    base = W.spiral_models()
+    base.tereg = abi.HXG_TEREG_EXPDISK
+    desc = W.grid_desc(n)
+    rng = np.random.Generator(np.random.PCG64(21))
+    dev = torch.device("cuda", 0)
+    b = [torch.tensor(rng.standard_normal(n ** 3) * 0.5e-6, dtype=torch.float64, device=dev)
+         for _ in range(3)]
+    ne = torch.tensor(0.01 * rng.standard_normal(n ** 3), dtype=torch.float64, device=dev)
+    maps = LOSMaps(obs, base, desc)
+    p0 = torch.tensor(params_of(maps.base), dtype=torch.float64, device=dev)
+    return maps, p0, b, ne
+
+
+def _loss_fn(maps, targets, weights):
+    def loss(p, b, ne):
+        outs = maps(p, b, ne)
+        tot = 0.
+        for o, t, w in zip(outs, targets, weights):
+            if o.numel():
+                tot = tot + (w * (o - t) ** 2).sum()
+        return tot
+    return loss
+
+
+def _richardson(f, x0, h):
+    """Central difference of f at x0 along a unit step, Richardson-extrapolated
+    from steps h and h/2."""
+    def cd(s):
+        return (f(x0 + s) - f(x0 - s)) / (2 * s)
+    return (4.0 * cd(0.5 * h) - cd(h)) / 3.0
+
+
+def _targets(maps, p0, b, ne):
+    with torch.no_grad():
+        pert = p0 * (1.0 + 0.01 * torch.tensor([1, -1, 1, 1, -1, 1, -1, 1], dtype=torch.float64,
+                                                device=p0.device))
+        outs = maps(pert, b, ne)
+    weights = []
+    for o in outs:
+        s = o.abs().max().item() if o.numel() else 1.0
+        weights.append(1.0 / (0.01 * s) ** 2 if s > 0 else 0.0)
+    return [o.clone() for o in outs], weights
+
+
+@pytest.mark.parametrize("freq", [23.0, 0.408])
+def test_adjoint_matches_finite_differences(freq):
+    maps, p0, b, ne = _setup(freq)
+    targets, weights = _targets(maps, p0, b, ne)
+    loss = _loss_fn(maps, targets, weights)
+    p = p0.clone().requires_grad_(True)
+    bb = [t.clone().requires_grad_(True) for t in b]
+    nn = ne.clone().requires_grad_(True)
+    L = loss(p, bb, nn)
+    L.backward()
+    gp = p.grad.cpu().numpy()
+    # parameters
+    for k in range(8):
+        def f_par(x, k=k):
+            pk = p0.clone()
+            pk[k] = x
+            with torch.no_grad():
+                return loss(pk, b, ne).item()
+        fd = _richardson(f_par, p0[k].item(), 1e-4 * abs(p0[k].item()))
+        scale = max(abs(fd), abs(gp[k]), 1e-30)
+        assert abs(gp[k] - fd) <= 2e-4 * scale + 1e-12 * abs(L.item()) / abs(p0[k].item()), \
+            (k, gp[k], fd)
+    # random voxels of the B and n_e grids
+    rng = np.random.Generator(np.random.PCG64(6))
+    grads = [t.grad for t in bb] + [nn.grad]
+    arrays = list(b) + [ne]
+    checked = 0
+    for comp in range(4):
+        g = grads[comp]
+        # probe the voxels with the largest gradients plus random ones
+        idx = list(torch.topk(g.abs(), 4).indices.cpu().numpy()) + \
+            list(rng.integers(0, g.numel(), 4))
+        rms = arrays[comp].std().item()
+        for i in idx:
+            def f_vox(x, comp=comp, i=i):
+                a = [t.clone() for t in arrays]
+                a[comp][i] = x
+                with torch.no_grad():
+                    return loss(p0, a[:3], a[3]).item()
+            fd = _richardson(f_vox, arrays[comp][i].item(), 1e-4 * rms)
+            an = g[i].item()
+            scale = max(abs(fd), abs(an))
+            if scale == 0:
+                continue
+            assert abs(an - fd) <= 2e-4 * scale + 1e-9 * abs(g).max().item(), \
+                (comp, int(i), an, fd)
+            checked += 1
+    assert checked >= 16
+
+
+def test_adjoint_cost_and_state_errors():
+    maps, p0, b, ne = _setup(1.4)
+    from hammurabix_b200 import _lib
+    integ = maps.integ
+    with pytest.raises(_lib.HxgError) as e:
+        integ.adjoint_device(maps.obs)     # no checkpointed forward yet
+    assert e.value.status == abi.HXG_ERR_STATE

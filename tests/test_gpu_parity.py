@@ -19,6 +19,13 @@ pytestmark = pytest.mark.gpu
 
 TOL64 = {"dm": 1e-10, "fd": 1e-10, "is": 1e-9, "qs": 1e-9, "us": 1e-9}
 TOL32 = 1e-5
+# FP32-compensated form on the strong-rotation stress case (0.408 GHz, 0.05 kpc
+# steps: ~600 samples through thousands of radians of Faraday rotation).  The
+# FP32 trilinear interpolation of the gridded n_e and B rounds each sample by
+# ~1 ulp at random; the running Faraday phase random-walks that into
+# ~1e-5 of Q/U.  On 0.01-kpc steps (five times the samples, a fifth of the
+# phase per sample) the same form stays below TOL32.
+TOL32_STRONG = 3e-5
 
 
 def _run_gpu(precision, passes, m, grids, mask):
@@ -153,7 +160,7 @@ def test_gpu_fp64_two_geometries_vs_oracle(oracle):
 
 # ---- FP32-compensated form vs the FP64 oracle ---------------------------------
 
-def _check_fp32c(oracle, passes, m, grids, mask):
+def _check_fp32c(oracle, passes, m, grids, mask, tol=TOL32):
     outs = _run_gpu("fp32c", passes, m, grids, mask)
     errs = {}
     for o, got in zip(passes, outs):
@@ -164,7 +171,7 @@ def _check_fp32c(oracle, passes, m, grids, mask):
                 continue
             errs[k] = max(errs.get(k, 0.0), rel_err(v, ref[k]))
     for k, e in errs.items():
-        assert e <= TOL32, (k, e, errs)
+        assert e <= tol, (k, e, errs)
     return errs
 
 
@@ -174,7 +181,28 @@ def test_gpu_fp32c_config1(oracle):
 
 def test_gpu_fp32c_grids(oracle, fields32):
     _check_fp32c(oracle, *cases.case_grid_small(fields32))
-    _check_fp32c(oracle, *cases.case_grid_lowfreq(fields32))
+    _check_fp32c(oracle, *cases.case_grid_lowfreq(fields32), tol=TOL32_STRONG)
+
+
+def test_gpu_fp32c_vs_fp64_config3_steps():
+    """Config-3 sampling (0.01 kpc steps to 30 kpc, 0.408 / 1.4 / 30 GHz) at
+    Nside 8-64 on a 128^3 random grid: FP32-compensated vs the FP64 form."""
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    bx, by, bz, ne = W.random_grids_torch(128, 3, 4, device=dev)
+    f64 = [t.double().reshape(-1).contiguous() for t in (bx, by, bz, ne)]
+    passes = W.config_grid([8, 16, 32, 64], 30.0, 0.01, [0.408, 1.4, 30.0])
+    res = {}
+    for prec in ("fp64", "fp32c"):
+        with I.Integrator(prec) as integ:
+            integ.set_models(W.grid_models())
+            integ.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(128), f64[:3])
+            integ.upload_grid_device(abi.HXG_FIELD_TEREG, W.grid_desc(128), f64[3:])
+            res[prec] = [integ.write_grid(o) for o in passes]
+    for a, b in zip(res["fp32c"], res["fp64"]):
+        for k, v in a.items():
+            if v is not None:
+                assert rel_err(v, b[k]) <= TOL32, (k, rel_err(v, b[k]))
 
 
 def test_gpu_fp32c_models_and_mask(oracle):
