@@ -163,8 +163,10 @@ shell_fp64_adjoint_kernel(const AdjointLaunch A) {
     long long acc_key = -1;
     double gt = P.em_gt, gpp = P.em_gp, last_index = nan("");
     double fdl = 0.;  // running FD of this chunk
-    const long long i0 = (P.step * c) >> P.log2_chunks;
-    const long long i1 = (P.step * (c + 1)) >> P.log2_chunks;
+    long long wlo, whi;
+    ray_window(P, ux, uy, uz, wlo, whi);
+    const long long i0 = max((P.step * c) >> P.log2_chunks, wlo);
+    const long long i1 = min((P.step * (c + 1)) >> P.log2_chunks, whi);
     for (long long i = i0; i < i1; ++i) {
       const double d = P.d_start + ((double)i + 0.5) * P.delta;
       const double px = ux * d + P.obs[0];

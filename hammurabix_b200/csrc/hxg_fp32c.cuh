@@ -193,8 +193,10 @@ shell_fp32c_kernel(const ShellLaunch P) {
     const double rc2_hi = 400. * M.kpc * M.kpc, rc2_lo = 9. * M.kpc * M.kpc;
     float last_index = __int_as_float(0x7fc00000), gt = float(P.em_gt),
           gp = float(P.em_gp), inv1mi = 1.f;
-    const long long i0 = (P.step * c) >> P.log2_chunks;
-    const long long i1 = (P.step * (c + 1)) >> P.log2_chunks;
+    long long wlo, whi;
+    ray_window(P, ux, uy, uz, wlo, whi);
+    const long long i0 = max((P.step * c) >> P.log2_chunks, wlo);
+    const long long i1 = min((P.step * (c + 1)) >> P.log2_chunks, whi);
     double d = P.d_start + ((double)i0 + 0.5) * P.delta;
     for (long long i = i0; i < i1; ++i, d += P.delta) {
       const double pz = fma(uz, d, oz);

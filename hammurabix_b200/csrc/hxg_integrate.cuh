@@ -66,6 +66,42 @@ struct ShellLaunch {
   FastModels fast;  // FP32C only
 };
 
+// Sample window [lo, hi) of one ray: the samples that can pass the
+// spherical |pos| <= r_max and vertical z_min <= z <= z_max cuts
+// (integrator.cc:179-182), from the roots of |o + u d|^2 = r_max^2 and
+// o_z + u_z d = z_min / z_max, widened by two samples on each side.  Samples
+// outside the window fail the cuts; every sample inside is still tested
+// exactly, so the window only saves the iterations that would be skipped.
+__device__ __forceinline__ void ray_window(const ShellLaunch &P, double ux,
+                                           double uy, double uz,
+                                           long long &lo, long long &hi) {
+  const double ox = P.obs[0], oy = P.obs[1], oz = P.obs[2];
+  const double b = ox * ux + oy * uy + oz * uz;  // o.u
+  const double c = (ox * ox + oy * oy + oz * oz) - P.gc_r_max * P.gc_r_max;
+  const double disc = b * b - c;
+  lo = 0;
+  hi = 0;
+  if (!(disc >= 0.)) return;  // the ray misses the r_max sphere
+  const double sq = sqrt(disc);
+  double da = -b - sq, db = -b + sq;
+  if (uz > 0.) {
+    da = fmax(da, (P.gc_z_min - oz) / uz);
+    db = fmin(db, (P.gc_z_max - oz) / uz);
+  } else if (uz < 0.) {
+    da = fmax(da, (P.gc_z_max - oz) / uz);
+    db = fmin(db, (P.gc_z_min - oz) / uz);
+  } else if (oz < P.gc_z_min || oz > P.gc_z_max) {
+    return;
+  }
+  if (!(da <= db)) return;
+  // d_i = d_start + (i + 1/2) delta
+  const double n = (double)P.step;
+  const double fa = fmin(fmax(floor((da - P.d_start) / P.delta - 0.5) - 2., 0.), n);
+  const double fb = fmin(fmax(ceil((db - P.d_start) / P.delta - 0.5) + 3., 0.), n);
+  lo = (long long)fa;
+  hi = (long long)fb;
+}
+
 // Kahan-compensated FP32 accumulator.
 struct KahanF {
   float s, c;
@@ -177,8 +213,10 @@ shell_fp64_kernel(const ShellLaunch P) {
     CellCache<double> cache;
     cache.key = -1;
     double last_index = nan(""), gt = P.em_gt, gp = P.em_gp;
-    const long long i0 = (P.step * c) >> P.log2_chunks;
-    const long long i1 = (P.step * (c + 1)) >> P.log2_chunks;
+    long long wlo, whi;
+    ray_window(P, ux, uy, uz, wlo, whi);
+    const long long i0 = max((P.step * c) >> P.log2_chunks, wlo);
+    const long long i1 = min((P.step * (c + 1)) >> P.log2_chunks, whi);
     for (long long i = i0; i < i1; ++i) {
       const double d = P.d_start + ((double)i + 0.5) * P.delta;
       const double px = ux * d + P.obs[0];
