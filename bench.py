@@ -253,6 +253,72 @@ def adjoint_ratio(args, dev, stream, torch):
             "samples": W.samples_of(o)}
 
 
+def batch_config5(args, dev, stream, torch):
+    """Config-5 batch: 256 parameter sets (seed 7: spiral b0 ~ U[2,8] muG,
+    pitch ~ U[-40,-5] deg, h_B ~ U[0.5,2] kpc) x 3 frequencies (0.408, 1.4,
+    30 GHz; the 30-GHz pass also makes DM and FD, as the reference pipeline
+    runs its last frequency first with them), 1-3 shells of Nside 64/128/256
+    to r_max ~ U[15,30] kpc at 0.01 kpc steps, one shared 256^3 FP32 random
+    grid.  One graph-captured batch (persistent shell kernel per shell
+    level, launch shape autotuned) against a loop of write_grid_device
+    calls over the same 768 passes."""
+    import numpy as np
+    from hammurabix_b200 import abi, workloads as W
+    from hammurabix_b200.integrator import Integrator
+    n = 256
+    bx, by, bz, ne = W.random_grids_torch(n, 5, 6, device=dev)
+    f64 = [t.double().reshape(-1).contiguous() for t in (bx, by, bz, ne)]
+    del bx, by, bz, ne
+    rng = np.random.Generator(np.random.PCG64(7))
+    entries = []
+    for _ in range(256):
+        m = W.grid_models(W.spiral_models(b0_muG=rng.uniform(2, 8), pitch_deg=rng.uniform(-40, -5),
+                                          hb_kpc=rng.uniform(0.5, 2)))
+        nsh = int(rng.integers(1, 4))
+        rmax = rng.uniform(15, 30)
+        for k, f in enumerate((30.0, 1.4, 0.408)):
+            o = W.make_obs([64 * 2 ** s for s in range(nsh)], rmax, 0.01, freq_ghz=f,
+                           do_dm=(k == 0), do_fd=(k == 0))
+            ndm, nfd, nsy = abi.obs_output_sizes(o)
+            z = lambda c: torch.zeros(c, dtype=torch.float64, device=dev) if c else None
+            entries.append((m, o, {"dm": z(ndm), "fd": z(nfd), "is": z(nsy), "qs": z(nsy),
+                                   "us": z(nsy)}))
+    ig = Integrator("fp32c")
+    ig.set_stream(stream.cuda_stream)
+    ig.set_models(entries[0][0])
+    ig.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(n), f64[:3])
+    ig.upload_grid_device(abi.HXG_FIELD_TEREG, W.grid_desc(n), f64[3:])
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, k):
+        fn()
+        torch.cuda.synchronize(dev)
+        ev[0].record(stream)
+        for _ in range(k):
+            fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize(dev)
+        return ev[0].elapsed_time(ev[1]) / k
+
+    def loop():
+        for m, o, d in entries:
+            ig.set_models(m)
+            ig.write_grid_device(o, d["dm"], d["fd"], d["is"], d["qs"], d["us"])
+
+    loop_ms = timed(loop, args.batch_steps)
+    b = ig.batch(entries, tune=True)
+    info = b.info()
+    batch_ms = timed(b.run, args.batch_steps)
+    b.close()
+    ig.close()
+    S = info["samples"]
+    return {"workload": "config5: 256 spiral parameter sets x 3 frequencies, 1-3 shells of "
+                        "Nside 64/128/256 to 15-30 kpc, 0.01 kpc steps, 256^3 FP32 grid, FP32C",
+            "passes": len(entries), "samples": S, "batch_ms": batch_ms, "loop_ms": loop_ms,
+            "batch_samples_per_s": S / (batch_ms / 1e3), "loop_samples_per_s": S / (loop_ms / 1e3),
+            "batch_speedup_vs_loop": loop_ms / batch_ms, "tuned_shape": info}
+
+
 def rel_err(a, b):
     d = (a - b).abs().max().item()
     s = b.abs().max().item()
@@ -270,6 +336,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=2)
+    ap.add_argument("--batch-steps", type=int, default=2)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -431,6 +498,12 @@ def main():
         adjoint = adjoint_ratio(args, dev, stream, torch)
         log(f"[rank {rank}] adjoint: {adjoint}")
 
+    # ---- config-5 batch: one graph vs a per-pass loop --------------------------
+    batch = None
+    if args.batch_steps > 0:
+        batch = batch_config5(args, dev, stream, torch)
+        log(f"[rank {rank}] batch: {batch}")
+
     # ---- roofline of the shell-integration kernel -------------------------------
     peak, peak_kind = measured_peaks()
     per_launch_s = kms / 1e3 / max(klaunch, 1)
@@ -478,6 +551,7 @@ def main():
             "fp32c_max_rel_err_vs_fp64": errs,
             "adjoint_fwd_ratio": adjoint["ratio"] if adjoint else None,
             "adjoint": adjoint,
+            "batch": batch,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

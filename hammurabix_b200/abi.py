@@ -144,6 +144,13 @@ class Obs(C.Structure):
                 ("sync_freq", _d)]
 
 
+class BatchEntry(C.Structure):
+    """hxg_batch_entry_t: one pass of a batch (models, obs, device outputs)."""
+    _fields_ = [("models", Models), ("obs", Obs),
+                ("d_dm", C.c_void_p), ("d_fd", C.c_void_p), ("d_is", C.c_void_p),
+                ("d_qs", C.c_void_p), ("d_us", C.c_void_p)]
+
+
 def npix(nside):
     return 12 * int(nside) * int(nside)
 

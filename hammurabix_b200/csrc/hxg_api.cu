@@ -18,6 +18,7 @@
 
 #include "../../include/hxg.h"
 #include "hxg_adjoint.cuh"
+#include "hxg_batch.cuh"
 #include "hxg_integrate.cuh"
 #include "hxg_internal.h"
 
@@ -372,12 +373,11 @@ int choose_chunks(const hxg_handle *h, uint64_t npix, uint64_t step) {
 }
 
 // All launch constants of one shell (integrator.cc:136-228 semantics).
-int build_launch(hxg_handle *h, const hxg_obs_t &o, uint32_t s,
-                 ShellLaunch &P, uint64_t &step_out) {
+int build_launch(hxg_handle *h, const hxg_models_t &m, const hxg_obs_t &o,
+                 uint32_t s, ShellLaunch &P, uint64_t &step_out) {
   const bool fp32 = h->precision == HXG_FP32C;
   const double L = fp32 ? 1.0 / cgs::kpc : 1.0;
   const double Bu = fp32 ? 1.0 / cgs::fp32_bunit : 1.0;
-  const hxg_models_t &m = h->models;
   std::memset(&P, 0, sizeof(P));
   double d_start, delta;
   uint64_t step;
@@ -577,7 +577,7 @@ int noalloc_shell_launch(const hxg_obs_t *o, const hxg_models_t *m,
     G.b_slots[0] = (m->breg == HXG_BREG_GRID || m->brnd == HXG_BRND_GRID) ? 0 : -1;
     G.t_slots[0] = (m->tereg == HXG_TEREG_GRID || m->ternd == HXG_TERND_GRID) ? 2 : -1;
   }
-  const int st = build_launch(&h, *o, s, *P, *step);
+  const int st = build_launch(&h, h.models, *o, s, *P, *step);
   h.groups.clear();  // the records belong to the caller
   return st;
 }
@@ -746,7 +746,7 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
   for (uint32_t s = 0; s < o->total_shell; ++s) {
     ShellLaunch P;
     uint64_t step;
-    if ((st = build_launch(h, *o, s, P, step)) != HXG_OK) return st;
+    if ((st = build_launch(h, h->models, *o, s, P, step)) != HXG_OK) return st;
     // inner-shell Faraday depth: the accumulated FD output map when it is
     // requested, otherwise an all-zero map (integrator.cc:78-86, 130-132)
     P.fdmap = o->do_fd ? d_fd : nullptr;
@@ -877,7 +877,7 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
   for (int s = (int)o->total_shell - 1; s >= 0; --s) {
     ShellLaunch F;
     uint64_t step;
-    if ((st = build_launch(h, *o, (uint32_t)s, F, step)) != HXG_OK) return st;
+    if ((st = build_launch(h, h->models, *o, (uint32_t)s, F, step)) != HXG_OK) return st;
     const int ns = (int)o->nside_shell[s];
     const uint64_t npix = npix_of((uint32_t)ns);
     for (int k = 0; k < 5; ++k)
@@ -1193,6 +1193,321 @@ int hxg_read_grid(hxg_handle *h, int field, uint64_t n, const double *pos,
     else
       out[i] = res[4 * i + 3];
   }
+  return HXG_OK;
+}
+
+}  // extern "C"
+
+// ===================================================================
+// batched forward
+// ===================================================================
+struct hxg_batch {
+  hxg_handle *h = nullptr;
+  std::vector<hxg_batch_entry_t> e;
+  int levels = 0;
+  bool fp32 = false;
+  int ngroups = 0;
+  int lanes = 1, grain = 4, tried = 0;
+  double best_ms = 0.;
+  int64_t samples = 0;
+  std::vector<size_t> tmp_off;  // per entry, doubles into tmp
+  std::vector<size_t> tmp_n;    // per entry, doubles per map
+  DevBuf tmp, zeros, zblocks, counters;
+  std::vector<DevBuf> plans, tiles, merges, mblocks;
+  std::vector<int> nplans, nmerge;
+  std::vector<unsigned long long> merge_blocks;
+  int nzero = 0;
+  unsigned long long zero_blocks = 0;
+  unsigned level_blocks = 0;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+using hxg::BatchLevel;
+using hxg::MergeJob;
+using hxg::ShellLaunch;
+using hxg::ZeroJob;
+
+bool reads_grid(const hxg_models_t &m, int which) {
+  switch (which) {
+    case 0: return m.breg == HXG_BREG_GRID;
+    case 1: return m.brnd == HXG_BRND_GRID;
+    case 2: return m.tereg == HXG_TEREG_GRID;
+    case 3: return m.ternd == HXG_TERND_GRID;
+    default: return m.cre == HXG_CRE_GRID;
+  }
+}
+
+template <typename T>
+int upload_vec(hxg_handle *h, DevBuf &b, const std::vector<T> &v) {
+  const size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
+  int st = ensure(h, b, bytes);
+  if (st != HXG_OK) return st;
+  if (!v.empty()) HXG_CK(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return HXG_OK;
+}
+
+// Device tables of a batch for one launch shape.
+int batch_tables(hxg_batch *b, int lanes, int grain) {
+  hxg_handle *h = b->h;
+  int st;
+  b->lanes = lanes;
+  b->grain = grain;
+  b->samples = 0;
+  double *tmp = static_cast<double *>(b->tmp.p);
+  for (int s = 0; s < b->levels; ++s) {
+    std::vector<ShellLaunch> P;
+    std::vector<unsigned long long> t0(1, 0ull);
+    std::vector<MergeJob> mj;
+    std::vector<unsigned long long> m0(1, 0ull);
+    for (size_t i = 0; i < b->e.size(); ++i) {
+      const hxg_batch_entry_t &E = b->e[i];
+      const hxg_obs_t &o = E.obs;
+      if ((uint32_t)s >= o.total_shell) continue;
+      ShellLaunch L;
+      uint64_t step;
+      if ((st = build_launch(h, E.models, o, (uint32_t)s, L, step)) != HXG_OK) return st;
+      L.fdmap = o.do_fd ? E.d_fd : nullptr;
+      L.nside_fdmap = o.do_fd ? (int)o.nside_fd : 0;
+      L.mask = nullptr;
+      double *t = tmp + b->tmp_off[i];
+      for (int k = 0; k < 5; ++k) L.out[k] = t + k * b->tmp_n[i];
+      int C = std::min(lanes, 32);
+      while (C > 1 && step / (uint64_t)C < 16) C >>= 1;
+      L.chunks = C;
+      L.log2_chunks = hxg::hpx_ilog2((uint64_t)C);
+      const uint64_t npix = npix_of(o.nside_shell[s]);
+      P.push_back(L);
+      t0.push_back(t0.back() + (npix * C + 31) / 32);
+      b->samples += (int64_t)(npix * step);
+      const int ns = (int)o.nside_shell[s];
+      const auto job = [&](int nmaps, double *d0, double *d1, double *d2, int kk, uint32_t nd) {
+        MergeJob J{};
+        J.dst[0] = d0; J.dst[1] = d1; J.dst[2] = d2;
+        for (int q = 0; q < nmaps; ++q) J.src[q] = t + (kk + q) * b->tmp_n[i];
+        J.nmaps = nmaps;
+        J.nside_dst = (int)nd;
+        J.nside_src = ns;
+        mj.push_back(J);
+        m0.push_back(m0.back() + (npix_of(nd) + 255) / 256);
+      };
+      if (o.do_dm) job(1, E.d_dm, nullptr, nullptr, 0, o.nside_dm);
+      if (o.do_sync) job(3, E.d_is, E.d_qs, E.d_us, 2, o.nside_sync);
+      if (o.do_fd) job(1, E.d_fd, nullptr, nullptr, 1, o.nside_fd);
+    }
+    b->nplans[s] = (int)P.size();
+    b->nmerge[s] = (int)mj.size();
+    b->merge_blocks[s] = m0.back();
+    if ((st = upload_vec(h, b->plans[s], P)) != HXG_OK) return st;
+    if ((st = upload_vec(h, b->tiles[s], t0)) != HXG_OK) return st;
+    if ((st = upload_vec(h, b->merges[s], mj)) != HXG_OK) return st;
+    if ((st = upload_vec(h, b->mblocks[s], m0)) != HXG_OK) return st;
+  }
+  return HXG_OK;
+}
+
+void batch_drop_graph(hxg_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  b->exec = nullptr;
+}
+
+int batch_capture(hxg_batch *b) {
+  hxg_handle *h = b->h;
+  batch_drop_graph(b);
+  cudaStream_t s = h->stream;
+  HXG_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = hxg::launch_batch_zero(s, static_cast<const ZeroJob *>(b->zeros.p),
+                                         static_cast<const unsigned long long *>(b->zblocks.p),
+                                         b->nzero, b->zero_blocks);
+  unsigned long long *ctr = static_cast<unsigned long long *>(b->counters.p);
+  for (int l = 0; l < b->levels && e == cudaSuccess; ++l) {
+    e = cudaMemsetAsync(ctr + l, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) break;
+    BatchLevel B;
+    B.plans = static_cast<const ShellLaunch *>(b->plans[l].p);
+    B.tile_start = static_cast<const unsigned long long *>(b->tiles[l].p);
+    B.nplans = b->nplans[l];
+    B.grain = b->grain;
+    B.counter = ctr + l;
+    if (B.nplans > 0) e = hxg::launch_batch_level(s, b->fp32, b->ngroups, B, b->level_blocks);
+    if (e != cudaSuccess) break;
+    e = hxg::launch_batch_merge(s, static_cast<const MergeJob *>(b->merges[l].p),
+                                static_cast<const unsigned long long *>(b->mblocks[l].p),
+                                b->nmerge[l], b->merge_blocks[l]);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(s, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return cuda_fail(h, e != cudaSuccess ? e : e2, "batch graph capture");
+  }
+  const cudaError_t e3 = cudaGraphInstantiate(&b->exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e3 != cudaSuccess) {
+    b->exec = nullptr;
+    return cuda_fail(h, e3, "cudaGraphInstantiate");
+  }
+  return HXG_OK;
+}
+
+int batch_time(hxg_batch *b, double *ms) {
+  hxg_handle *h = b->h;
+  cudaEvent_t e0, e1;
+  HXG_CK(cudaEventCreate(&e0));
+  HXG_CK(cudaEventCreate(&e1));
+  cudaError_t e = cudaGraphLaunch(b->exec, h->stream);  // warm-up
+  if (e == cudaSuccess) e = cudaEventRecord(e0, h->stream);
+  if (e == cudaSuccess) e = cudaGraphLaunch(b->exec, h->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(e1, h->stream);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  float f = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&f, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return cuda_fail(h, e, "batch timing run");
+  *ms = f;
+  return HXG_OK;
+}
+
+void batch_free(hxg_batch *b) {
+  batch_drop_graph(b);
+  DevBuf *bufs[] = {&b->tmp, &b->zeros, &b->zblocks, &b->counters};
+  for (DevBuf *d : bufs)
+    if (d->p) cudaFree(d->p);
+  for (auto *v : {&b->plans, &b->tiles, &b->merges, &b->mblocks})
+    for (DevBuf &d : *v)
+      if (d.p) cudaFree(d.p);
+}
+
+}  // namespace
+
+extern "C" {
+
+int hxg_batch_create(hxg_handle *h, int n, const hxg_batch_entry_t *entries,
+                     int tune, hxg_batch **out) {
+  if (!h || !out || n < 1 || !entries) return HXG_ERR_INVALID;
+  *out = nullptr;
+  cudaSetDevice(h->device);
+  if (!h->have_models) return fail(h, HXG_ERR_STATE, "models not set");
+  int st;
+  for (int i = 0; i < n; ++i) {
+    const hxg_batch_entry_t &E = entries[i];
+    if ((st = validate_obs(h, &E.obs)) != HXG_OK) return st;
+    if (E.obs.do_mask) return fail(h, HXG_ERR_UNSUPPORTED, "entry %d: masks are not batched", i);
+    for (int w = 0; w < 5; ++w)
+      if (reads_grid(E.models, w) != reads_grid(h->models, w))
+        return fail(h, HXG_ERR_INVALID,
+                    "entry %d reads other fields from grids than the handle's models", i);
+    if (E.obs.do_sync && E.models.cre == HXG_CRE_NONE)
+      return fail(h, HXG_ERR_INVALID, "entry %d: synchrotron output needs a CRE model", i);
+    if ((E.obs.do_dm && !E.d_dm) || (E.obs.do_fd && !E.d_fd) ||
+        (E.obs.do_sync && (!E.d_is || !E.d_qs || !E.d_us)))
+      return fail(h, HXG_ERR_INVALID, "entry %d: an output requested by obs is NULL", i);
+    std::string why;
+    if (!models_supported(E.models, &why))
+      return fail(h, HXG_ERR_UNSUPPORTED, "entry %d: %s", i, why.c_str());
+  }
+  if ((st = build_groups(h)) != HXG_OK) return st;
+  hxg_batch *b = new hxg_batch();
+  b->h = h;
+  b->e.assign(entries, entries + n);
+  b->fp32 = h->precision == HXG_FP32C;
+  b->ngroups = (int)h->groups.size();
+  size_t total = 0;
+  std::vector<ZeroJob> zj;
+  std::vector<unsigned long long> z0(1, 0ull);
+  for (const hxg_batch_entry_t &E : b->e) {
+    uint32_t mx = 0;
+    for (uint32_t s = 0; s < E.obs.total_shell; ++s) mx = std::max(mx, E.obs.nside_shell[s]);
+    b->levels = std::max(b->levels, (int)E.obs.total_shell);
+    b->tmp_off.push_back(total);
+    b->tmp_n.push_back(npix_of(mx));
+    total += 5 * npix_of(mx);
+    const auto zero = [&](double *p, uint32_t ns) {
+      zj.push_back(ZeroJob{p, npix_of(ns)});
+      z0.push_back(z0.back() + (npix_of(ns) + 255) / 256);
+    };
+    if (E.obs.do_dm) zero(E.d_dm, E.obs.nside_dm);
+    if (E.obs.do_fd) zero(E.d_fd, E.obs.nside_fd);
+    if (E.obs.do_sync) {
+      zero(E.d_is, E.obs.nside_sync);
+      zero(E.d_qs, E.obs.nside_sync);
+      zero(E.d_us, E.obs.nside_sync);
+    }
+  }
+  b->nzero = (int)zj.size();
+  b->zero_blocks = z0.back();
+  b->plans.resize(b->levels);
+  b->tiles.resize(b->levels);
+  b->merges.resize(b->levels);
+  b->mblocks.resize(b->levels);
+  b->nplans.assign(b->levels, 0);
+  b->nmerge.assign(b->levels, 0);
+  b->merge_blocks.assign(b->levels, 0ull);
+  const auto bail = [&](int code) {
+    batch_free(b);
+    delete b;
+    return code;
+  };
+  if ((st = ensure(h, b->tmp, total * sizeof(double))) != HXG_OK) return bail(st);
+  if ((st = ensure(h, b->counters, b->levels * sizeof(unsigned long long))) != HXG_OK)
+    return bail(st);
+  if ((st = upload_vec(h, b->zeros, zj)) != HXG_OK) return bail(st);
+  if ((st = upload_vec(h, b->zblocks, z0)) != HXG_OK) return bail(st);
+  int per_sm = 0;
+  cudaError_t ce = hxg::batch_level_occupancy(b->fp32, b->ngroups, &per_sm);
+  if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "occupancy"));
+  b->level_blocks = (unsigned)std::max(1, per_sm) * (unsigned)h->sm_count;
+  // launch shapes: lanes per pixel x tiles per work fetch
+  const int shapes[][2] = {{1, 4}, {2, 4}, {4, 4}, {8, 4}, {1, 16}, {2, 1}};
+  int best = 0;
+  if (tune) {
+    double best_ms = 1e300;
+    for (int k = 0; k < (int)(sizeof(shapes) / sizeof(shapes[0])); ++k) {
+      if ((st = batch_tables(b, shapes[k][0], shapes[k][1])) != HXG_OK) return bail(st);
+      if ((st = batch_capture(b)) != HXG_OK) return bail(st);
+      double ms;
+      if ((st = batch_time(b, &ms)) != HXG_OK) return bail(st);
+      ++b->tried;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = k;
+      }
+    }
+    b->best_ms = best_ms;
+  }
+  if ((st = batch_tables(b, shapes[best][0], shapes[best][1])) != HXG_OK) return bail(st);
+  if ((st = batch_capture(b)) != HXG_OK) return bail(st);
+  *out = b;
+  return HXG_OK;
+}
+
+int hxg_batch_run(hxg_batch *b) {
+  if (!b || !b->exec) return HXG_ERR_INVALID;
+  hxg_handle *h = b->h;
+  cudaSetDevice(h->device);
+  HXG_CK(cudaGraphLaunch(b->exec, h->stream));
+  h->launch_count += 1 + 2 * b->levels;
+  return HXG_OK;
+}
+
+int hxg_batch_info(const hxg_batch *b, int *lanes_per_pixel, int *grain,
+                   int *tried, double *best_ms, int64_t *samples) {
+  if (!b) return HXG_ERR_INVALID;
+  if (lanes_per_pixel) *lanes_per_pixel = b->lanes;
+  if (grain) *grain = b->grain;
+  if (tried) *tried = b->tried;
+  if (best_ms) *best_ms = b->best_ms;
+  if (samples) *samples = b->samples;
+  return HXG_OK;
+}
+
+int hxg_batch_destroy(hxg_batch *b) {
+  if (!b) return HXG_ERR_INVALID;
+  cudaSetDevice(b->h->device);
+  batch_free(b);
+  delete b;
   return HXG_OK;
 }
 

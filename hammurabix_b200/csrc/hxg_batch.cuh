@@ -1,0 +1,87 @@
+// hxg_batch.cuh -- batched forward: many independent passes (parameter
+// sets x frequencies) of Integrator::write_grid (integrator.cc:23-134) in
+// one CUDA graph.  Per shell level the graph holds one persistent shell
+// kernel over every entry that has that shell and one kernel that merges
+// the shell maps into each entry's outputs (Hampix::accumulate,
+// hamdis.h:698-721); the outer-shell levels read the inner Faraday depth
+// the earlier levels accumulated (integrator.cc:78-86).
+#pragma once
+
+#include "hxg_fp32c.cuh"
+#include "hxg_integrate.cuh"
+
+namespace hxg {
+
+// One shell level of a batch: plan k (one entry's shell launch block) owns
+// the warp tiles [tile_start[k], tile_start[k + 1]).  Warps take `grain`
+// tiles at a time from the work counter (zeroed before the launch).
+struct BatchLevel {
+  const ShellLaunch *plans;
+  const unsigned long long *tile_start;  // nplans + 1 entries
+  int nplans;
+  int grain;
+  unsigned long long *counter;
+};
+
+template <int NG, bool kFp32>
+__device__ __forceinline__ void batch_level_body(const BatchLevel &B) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long total = B.tile_start[B.nplans];
+  for (;;) {
+    unsigned long long t0 = 0;
+    if (lane == 0) t0 = atomicAdd(B.counter, (unsigned long long)B.grain);
+    t0 = __shfl_sync(0xffffffffu, t0, 0);
+    if (t0 >= total) return;
+    const unsigned long long t1 = min(t0 + (unsigned long long)B.grain, total);
+    // last plan whose first tile is <= t0
+    int lo = 0, hi = B.nplans - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (B.tile_start[mid] <= t0) lo = mid; else hi = mid - 1;
+    }
+    int k = lo;
+    for (unsigned long long t = t0; t < t1; ++t) {
+      while (t >= B.tile_start[k + 1]) ++k;
+      const ShellLaunch &P = B.plans[k];
+      const long long gw = (long long)(t - B.tile_start[k]);
+      if (kFp32)
+        fp32c_tile<NG>(P, gw, lane);
+      else
+        fp64_tile<NG, false>(P, gw, lane);
+    }
+  }
+}
+
+// The launch blocks are read from global memory, which needs more live
+// registers than the single-launch kernel: 2 resident blocks per SM.
+template <int NG>
+__global__ void __launch_bounds__(256, 2)
+batch_fp32c_kernel(const BatchLevel B) {
+  batch_level_body<NG, true>(B);
+}
+
+template <int NG>
+__global__ void __launch_bounds__(256)
+batch_fp64_kernel(const BatchLevel B) {
+  batch_level_body<NG, false>(B);
+}
+
+// Map merges of one level: job j adds nmaps shell maps at nside_src into
+// outputs at nside_dst (directly when the Nsides agree, else by HEALPix
+// interpolation at each output pixel); it owns blocks
+// [block0[j], block0[j + 1]).
+struct MergeJob {
+  double *dst[3];
+  const double *src[3];
+  int nmaps, nside_dst, nside_src, _pad;
+};
+
+// Zeroing of every output map of the batch (Grid_obs maps start at zero,
+// grid_obs.cc:21-43): job j clears n doubles at p with blocks
+// [block0[j], block0[j + 1]).
+struct ZeroJob {
+  double *p;
+  unsigned long long n;
+};
+
+}  // namespace hxg

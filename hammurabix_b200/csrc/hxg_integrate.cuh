@@ -173,12 +173,11 @@ __device__ __forceinline__ void ipa2(T xv, T yv, T &c2, T &s2) {
 // ===================================================================
 // FP64 parity form
 // ===================================================================
+// Warp gw of shell launch P (32/C pixels, C lanes each).  All 32 lanes of
+// the warp call it with the same gw.
 template <int NG, bool kCache>
-__global__ void __launch_bounds__(256)
-shell_fp64_kernel(const ShellLaunch P) {
-  const int lane = threadIdx.x & 31;
-  const long long gw =
-      ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
+                                          int lane) {
   const int C = P.chunks;
   const int seg = lane >> P.log2_chunks;
   const int c = lane & (C - 1);
@@ -304,6 +303,13 @@ shell_fp64_kernel(const ShellLaunch P) {
     if (P.do_fd || P.do_sync) P.out[1][ring] = 0.;
     if (P.do_sync) P.out[2][ring] = P.out[3][ring] = P.out[4][ring] = 0.;
   }
+}
+
+template <int NG, bool kCache>
+__global__ void __launch_bounds__(256)
+shell_fp64_kernel(const ShellLaunch P) {
+  fp64_tile<NG, kCache>(P, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                        threadIdx.x & 31);
 }
 
 }  // namespace hxg

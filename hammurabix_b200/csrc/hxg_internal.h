@@ -11,6 +11,9 @@ namespace hxg {
 struct ShellLaunch;
 struct DevGridGroup;
 struct AdjointLaunch;
+struct BatchLevel;
+struct MergeJob;
+struct ZeroJob;
 
 cudaError_t launch_accumulate(cudaStream_t s, int nside_dst, int nside_src,
                               int nmaps, double *const *dst,
@@ -38,6 +41,15 @@ cudaError_t launch_accumulate_transpose(cudaStream_t s, int nside_out,
                                         double *g_shell, double scale);
 cudaError_t launch_adjoint(cudaStream_t s, const AdjointLaunch &A,
                            unsigned blocks, unsigned threads);
+cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups,
+                               const BatchLevel &B, unsigned blocks);
+cudaError_t batch_level_occupancy(bool fp32, int ngroups, int *blocks_per_sm);
+cudaError_t launch_batch_merge(cudaStream_t s, const MergeJob *jobs,
+                               const unsigned long long *block0, int njobs,
+                               unsigned long long nblocks);
+cudaError_t launch_batch_zero(cudaStream_t s, const ZeroJob *jobs,
+                              const unsigned long long *block0, int njobs,
+                              unsigned long long nblocks);
 cudaError_t launch_unpack_grad(cudaStream_t s, uint64_t n, const double *rec,
                                double *gbx, double *gby, double *gbz,
                                double *gne);

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "hxg_adjoint.cuh"
+#include "hxg_batch.cuh"
 #include "hxg_fp32c.cuh"
 #include "hxg_integrate.cuh"
 #include "hxg_internal.h"
@@ -167,6 +168,53 @@ __global__ void unpack_grad_kernel(uint64_t n, const double *rec, double *gbx,
 }
 
 // ---- launch wrappers -----------------------------------------------------
+// Block b of a job-table kernel belongs to the last job j with
+// block0[j] <= b (block0 has njobs + 1 entries).
+__device__ __forceinline__ int job_of_block(const unsigned long long *block0,
+                                            int njobs) {
+  __shared__ int sj;
+  if (threadIdx.x == 0) {
+    const unsigned long long b = blockIdx.x;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (block0[mid] <= b) lo = mid; else hi = mid - 1;
+    }
+    sj = lo;
+  }
+  __syncthreads();
+  return sj;
+}
+
+__global__ void batch_merge_kernel(const MergeJob *jobs,
+                                   const unsigned long long *block0,
+                                   int njobs) {
+  const int j = job_of_block(block0, njobs);
+  const MergeJob &J = jobs[j];
+  const Hpx hd = hpx_make((uint64_t)J.nside_dst);
+  const uint64_t i = (blockIdx.x - block0[j]) * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= hd.npix) return;
+  if (J.nside_dst == J.nside_src) {
+    for (int k = 0; k < J.nmaps; ++k) J.dst[k][i] = J.dst[k][i] + J.src[k][i];
+    return;
+  }
+  const Hpx hs = hpx_make((uint64_t)J.nside_src);
+  double th, ph;
+  hpx_pix2ang(hd, i, th, ph);
+  uint64_t pix[4];
+  double w[4];
+  hpx_interp_weights(hs, th, ph, pix, w);
+  for (int k = 0; k < J.nmaps; ++k)
+    J.dst[k][i] = J.dst[k][i] + hpx_interp_apply(J.src[k], pix, w);
+}
+
+__global__ void batch_zero_kernel(const ZeroJob *jobs,
+                                  const unsigned long long *block0, int njobs) {
+  const int j = job_of_block(block0, njobs);
+  const uint64_t i = (blockIdx.x - block0[j]) * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < jobs[j].n) jobs[j].p[i] = 0.;
+}
+
 static inline unsigned blocks_for(uint64_t n, unsigned tpb) {
   return (unsigned)((n + tpb - 1) / tpb);
 }
@@ -248,6 +296,55 @@ cudaError_t launch_shell(cudaStream_t s, bool fp32, const ShellLaunch &P,
     else
       shell_fp64_kernel<4, false><<<blocks, threads, 0, s>>>(P);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups,
+                               const BatchLevel &B, unsigned blocks) {
+  if (fp32) {
+    if (ngroups == 0)
+      batch_fp32c_kernel<0><<<blocks, 256, 0, s>>>(B);
+    else if (ngroups == 1)
+      batch_fp32c_kernel<1><<<blocks, 256, 0, s>>>(B);
+    else
+      batch_fp32c_kernel<4><<<blocks, 256, 0, s>>>(B);
+  } else {
+    if (ngroups == 0)
+      batch_fp64_kernel<0><<<blocks, 256, 0, s>>>(B);
+    else if (ngroups == 1)
+      batch_fp64_kernel<1><<<blocks, 256, 0, s>>>(B);
+    else
+      batch_fp64_kernel<4><<<blocks, 256, 0, s>>>(B);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t batch_level_occupancy(bool fp32, int ngroups, int *blocks_per_sm) {
+  const void *f;
+  if (fp32)
+    f = ngroups == 0 ? (const void *)batch_fp32c_kernel<0>
+        : ngroups == 1 ? (const void *)batch_fp32c_kernel<1>
+                       : (const void *)batch_fp32c_kernel<4>;
+  else
+    f = ngroups == 0 ? (const void *)batch_fp64_kernel<0>
+        : ngroups == 1 ? (const void *)batch_fp64_kernel<1>
+                       : (const void *)batch_fp64_kernel<4>;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, 256, 0);
+}
+
+cudaError_t launch_batch_merge(cudaStream_t s, const MergeJob *jobs,
+                               const unsigned long long *block0, int njobs,
+                               unsigned long long nblocks) {
+  if (njobs == 0 || nblocks == 0) return cudaSuccess;
+  batch_merge_kernel<<<(unsigned)nblocks, 256, 0, s>>>(jobs, block0, njobs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_zero(cudaStream_t s, const ZeroJob *jobs,
+                              const unsigned long long *block0, int njobs,
+                              unsigned long long nblocks) {
+  if (njobs == 0 || nblocks == 0) return cudaSuccess;
+  batch_zero_kernel<<<(unsigned)nblocks, 256, 0, s>>>(jobs, block0, njobs);
   return cudaGetLastError();
 }
 

@@ -113,6 +113,14 @@ class Integrator:
             self._h, C.byref(obs), ptr(g_dm), ptr(g_fd), ptr(g_is), ptr(g_qs), ptr(g_us),
             ptr(grad_params), ptr(gb[0]), ptr(gb[1]), ptr(gb[2]), ptr(grad_ne)), self._h)
 
+    # ---- batched forward ---------------------------------------------------
+    def batch(self, entries, tune=False):
+        """Plan a batch of independent passes sharing this handle's grids.
+        entries: iterable of (models, obs, outs) with outs a dict of torch
+        CUDA float64 tensors keyed "dm", "fd", "is", "qs", "us" (the ones
+        obs requests).  Returns a Batch; Batch.run() launches its graph."""
+        return Batch(self, list(entries), tune)
+
     # ---- timing ----------------------------------------------------------
     def set_timing(self, enable=True):
         _lib.check(self._lib.hxg_set_timing(self._h, int(bool(enable))), self._h)
@@ -141,6 +149,50 @@ class Integrator:
 
 
 # ---- stateless device helpers (known-answer entry points) -----------------
+
+class Batch:
+    """A planned batch (hxg_batch_create): one CUDA graph per run."""
+
+    def __init__(self, integ, entries, tune):
+        self._lib = integ._lib
+        self._integ = integ
+        arr = (abi.BatchEntry * len(entries))()
+        self._keep = []
+        for k, (models, obs, outs) in enumerate(entries):
+            arr[k].models = models
+            arr[k].obs = obs
+            for key, field in (("dm", "d_dm"), ("fd", "d_fd"), ("is", "d_is"), ("qs", "d_qs"),
+                               ("us", "d_us")):
+                t = outs.get(key)
+                if t is not None:
+                    self._keep.append(t)
+                    setattr(arr[k], field, t.data_ptr())
+        self._b = C.c_void_p()
+        _lib.check(self._lib.hxg_batch_create(integ._h, len(entries), arr, int(bool(tune)),
+                                              C.byref(self._b)), integ._h)
+
+    def run(self):
+        _lib.check(self._lib.hxg_batch_run(self._b), self._integ._h)
+
+    def info(self):
+        lanes, grain, tried = C.c_int(), C.c_int(), C.c_int()
+        ms, samples = C.c_double(), C.c_int64()
+        _lib.check(self._lib.hxg_batch_info(self._b, C.byref(lanes), C.byref(grain),
+                                            C.byref(tried), C.byref(ms), C.byref(samples)))
+        return {"lanes_per_pixel": lanes.value, "grain": grain.value, "shapes_tried": tried.value,
+                "best_ms": ms.value, "samples": samples.value}
+
+    def close(self):
+        if self._b:
+            self._lib.hxg_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
 
 def pix2ang(nside):
     lib = _lib.load()

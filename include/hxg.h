@@ -279,6 +279,43 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *obs,
                        double *d_grad_bx, double *d_grad_by,
                        double *d_grad_bz, double *d_grad_ne);
 
+/* ---- batched forward ---------------------------------------------------
+ * Many independent passes -- parameter sets x frequencies, each one
+ * Integrator::write_grid call (source/integrator/integrator.cc:23-134)
+ * with its own models and hxg_obs_t -- planned once and run as one CUDA
+ * graph.  The reference has no batch entry point; a caller loops over
+ * Pipeline runs (source/pipeline/pipeline.cc:165-190).
+ *
+ *  - every entry shares the handle's grids and precision, and its models
+ *    must read the same fields from grids as the handle's models (the
+ *    analytic parameters may differ); masks are not supported;
+ *  - outputs are the caller's device maps (RING), distinct per entry;
+ *  - the plan holds per-entry shell temporaries and launch blocks and a
+ *    graph with, per shell level, one persistent shell kernel over all
+ *    entries (warps take pixel tiles from a work counter) and one kernel
+ *    that merges the shell maps into the outputs; an entry's outer shells
+ *    read the Faraday depth its inner shells accumulated, as in
+ *    write_grid;
+ *  - tune != 0: the launch shapes (lanes per pixel x tiles per fetch) are
+ *    timed once in hxg_batch_create and the fastest is kept;
+ *  - hxg_batch_run launches the graph on the handle's stream and does not
+ *    synchronise; the entries' host data are not read again.             */
+typedef struct {
+  hxg_models_t models;
+  hxg_obs_t obs;
+  double *d_dm, *d_fd, *d_is, *d_qs, *d_us;
+} hxg_batch_entry_t;
+typedef struct hxg_batch hxg_batch;
+int hxg_batch_create(hxg_handle *h, int n, const hxg_batch_entry_t *entries,
+                     int tune, hxg_batch **out);
+int hxg_batch_run(hxg_batch *b);
+/* Launch shape in use (lanes per pixel, tiles per fetch), the number of
+ * shapes timed and the best graph time (ms; 0 without tuning), and the
+ * LOS samples one run covers.                                             */
+int hxg_batch_info(const hxg_batch *b, int *lanes_per_pixel, int *grain,
+                   int *tried, double *best_ms, int64_t *samples);
+int hxg_batch_destroy(hxg_batch *b);
+
 /* ---- timing of the integration kernels ------------------------------
  * enable != 0: every shell-integration launch is bracketed by CUDA events
  * on the launching stream.  hxg_get_timing returns the summed device time

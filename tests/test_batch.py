@@ -1,0 +1,95 @@
+"""Batched forward (hxg_batch_create / hxg_batch_run): a batch of passes with
+different spiral parameters, shell layouts, LOS lengths and frequencies,
+run as one CUDA graph, against the same passes run one write_grid_device
+call at a time on the same handle.  The batch may split pixels over a
+different number of lanes than the single call, which changes the summation
+order: FP64 agrees to the parity tolerance (1e-10), FP32C to 1e-5."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from hammurabix_b200 import _lib, abi, units as U, workloads as W
+from hammurabix_b200 import integrator as I
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _entries(rng, n):
+    out = []
+    for k in range(n):
+        m = W.grid_models(W.spiral_models(b0_muG=rng.uniform(2, 8),
+                                          pitch_deg=rng.uniform(-40, -5),
+                                          hb_kpc=rng.uniform(0.5, 2)))
+        nsh = int(rng.integers(1, 4))
+        nsides = [8 * 2 ** s for s in range(nsh)]
+        freq = [0.408, 1.4, 30.0][k % 3]
+        o = W.make_obs(nsides, rng.uniform(15, 30), 0.05, freq_ghz=freq,
+                       do_dm=(k % 3 == 0), do_fd=(k % 3 == 0))
+        out.append((m, o))
+    return out
+
+
+def _outs(o, dev):
+    ndm, nfd, nsy = abi.obs_output_sizes(o)
+    z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev) if n else None
+    return {"dm": z(ndm), "fd": z(nfd), "is": z(nsy), "qs": z(nsy), "us": z(nsy)}
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32c", 1e-5)])
+def test_batch_matches_per_entry_loop(fields32, precision, tol):
+    dev = torch.device("cuda", 0)
+    rng = np.random.Generator(np.random.PCG64(7))
+    ents = _entries(rng, 9)
+    bx, by, bz, ne = (torch.tensor(np.asarray(a, dtype=np.float64).reshape(-1), device=dev)
+                      for a in fields32)
+    with I.Integrator(precision) as integ:
+        integ.set_models(ents[0][0])
+        integ.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(32), [bx, by, bz])
+        integ.upload_grid_device(abi.HXG_FIELD_TEREG, W.grid_desc(32), [ne])
+        ref = []
+        for m, o in ents:
+            integ.set_models(m)
+            outs = _outs(o, dev)
+            integ.write_grid_device(o, outs["dm"], outs["fd"], outs["is"], outs["qs"], outs["us"])
+            ref.append(outs)
+        integ.sync()
+        got = [_outs(o, dev) for _, o in ents]
+        b = integ.batch([(m, o, g) for (m, o), g in zip(ents, got)], tune=(precision == "fp32c"))
+        for _ in range(2):      # a second run starts from zeroed outputs again
+            b.run()
+        integ.sync()
+        info = b.info()
+        b.close()
+    assert info["samples"] > 0
+    if precision == "fp32c":
+        assert info["shapes_tried"] > 1 and info["best_ms"] > 0
+    for k, (r, g) in enumerate(zip(ref, got)):
+        for key, t in r.items():
+            if t is None:
+                continue
+            e = rel_err(g[key].cpu().numpy(), t.cpu().numpy())
+            assert e <= tol, (k, key, e)
+            assert t.abs().max().item() > 0 or key == "fd"
+
+
+def test_batch_rejects_mismatched_grid_reads_and_masks(fields32):
+    dev = torch.device("cuda", 0)
+    rng = np.random.Generator(np.random.PCG64(8))
+    (m, o), = _entries(rng, 1)
+    bx, by, bz, ne = (torch.tensor(np.asarray(a, dtype=np.float64).reshape(-1), device=dev)
+                      for a in fields32)
+    with I.Integrator("fp32c") as integ:
+        integ.set_models(m)
+        integ.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(32), [bx, by, bz])
+        integ.upload_grid_device(abi.HXG_FIELD_TEREG, W.grid_desc(32), [ne])
+        other = abi.Models.from_buffer_copy(m)
+        other.brnd = abi.HXG_BRND_NONE
+        with pytest.raises(_lib.HxgError) as e:
+            integ.batch([(other, o, _outs(o, dev))])
+        assert e.value.status == abi.HXG_ERR_INVALID
+        masked = abi.Obs.from_buffer_copy(o)
+        masked.do_mask = 1
+        with pytest.raises(_lib.HxgError) as e:
+            integ.batch([(m, masked, _outs(o, dev))])
+        assert e.value.status == abi.HXG_ERR_UNSUPPORTED
