@@ -41,8 +41,9 @@ WORKLOADS = {
                   freqs_ghz=[0.408, 1.4, 30.0], grid_n=128, seeds=(3, 4),
                   cpu_sample_shells=[4, 8, 16, 32]),
     # the case kernel captures run on: grid records (268 MB FP32) above L2,
-    # a few ms per launch
-    "profile": dict(nside_shells=[16, 32, 64, 128], r_max_kpc=30.0, res_kpc=0.01,
+    # an Nside-512 outer shell (one lane per pixel, as the config-3 outer
+    # shells), about 15 ms per launch
+    "profile": dict(nside_shells=[64, 128, 256, 512], r_max_kpc=30.0, res_kpc=0.01,
                     freqs_ghz=[0.408, 1.4, 30.0], grid_n=256, seeds=(3, 4),
                     cpu_sample_shells=[4, 8, 16, 32]),
 }

@@ -1393,8 +1393,8 @@ int hxg_batch_create(hxg_handle *h, int n, const hxg_batch_entry_t *entries,
   int st;
   for (int i = 0; i < n; ++i) {
     const hxg_batch_entry_t &E = entries[i];
-    if ((st = validate_obs(h, &E.obs)) != HXG_OK) return st;
     if (E.obs.do_mask) return fail(h, HXG_ERR_UNSUPPORTED, "entry %d: masks are not batched", i);
+    if ((st = validate_obs(h, &E.obs)) != HXG_OK) return st;
     for (int w = 0; w < 5; ++w)
       if (reads_grid(E.models, w) != reads_grid(h->models, w))
         return fail(h, HXG_ERR_INVALID,
