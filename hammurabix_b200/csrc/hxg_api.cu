@@ -134,7 +134,7 @@ bool models_supported(const hxg_models_t &m, std::string *why) {
   switch (m.breg) {
     case HXG_BREG_NONE: case HXG_BREG_GRID: case HXG_BREG_LSA:
     case HXG_BREG_UNIF: case HXG_BREG_CART: case HXG_BREG_HELIX:
-    case HXG_BREG_SPIRAL:
+    case HXG_BREG_SPIRAL: case HXG_BREG_JAFFE: case HXG_BREG_JF12:
       break;
     default:
       *why = "regular B model not supported on the device";
@@ -146,7 +146,7 @@ bool models_supported(const hxg_models_t &m, std::string *why) {
   }
   switch (m.tereg) {
     case HXG_TEREG_NONE: case HXG_TEREG_GRID: case HXG_TEREG_UNIF:
-    case HXG_TEREG_EXPDISK:
+    case HXG_TEREG_EXPDISK: case HXG_TEREG_YMW16:
       break;
     default:
       *why = "regular n_e model not supported on the device";
@@ -362,6 +362,80 @@ DevModels dev_models(const hxg_models_t &m, const double obs[3], double L,
     d.cre_unif_r0 = m.cre_unif.r0 * L;
   }
   d.cre_R0 = rsun * L;
+  // Breg_jaffe: the Param block in working units and its parameter-only
+  // constants (breg_jaffe.cc:14-17, 42-46, 107-108, 183-187)
+  {
+    JaffeDev &J = d.jaffe;
+    J.p = m.jaffe;
+    for (double *v : {&J.p.disk_amp, &J.p.halo_amp, &J.p.ring_amp, &J.p.bar_amp}) *v *= Bu;
+    for (int k = 0; k < 8; ++k) J.p.arm_amp[k] *= Bu;
+    for (double *v : {&J.p.disk_z0, &J.p.halo_z0, &J.p.r_inner, &J.p.r_scale, &J.p.r_peak,
+                      &J.p.ring_r, &J.p.bar_a, &J.p.bar_b, &J.p.arm_r0, &J.p.arm_z0,
+                      &J.p.comp_r, &J.p.comp_d})
+      *v *= L;
+    J.cos_p = std::cos(m.jaffe.arm_pitch);
+    J.sin_p = std::sin(m.jaffe.arm_pitch);
+    J.beta_inv = -J.sin_p / J.cos_p;
+    J.cos_b = std::cos(m.jaffe.bar_phi0);
+    J.sin_b = std::sin(m.jaffe.bar_phi0);
+    J.bar_lim = J.p.bar_a + 0.5 * J.p.comp_d;
+    J.c0 = 1. / m.jaffe.comp_c - 1.;
+    J.r_forbid = 0.5 * cgs::kpc * L;
+  }
+  // Breg_jf12 (breg_jf12.cc:10-62, 96-104)
+  {
+    Jf12Dev &F = d.jf12;
+    F.p = m.jf12;
+    for (double *v : {&F.p.b_arm1, &F.p.b_arm2, &F.p.b_arm3, &F.p.b_arm4, &F.p.b_arm5,
+                      &F.p.b_arm6, &F.p.b_arm7, &F.p.b_ring, &F.p.Bn, &F.p.Bs, &F.p.B0_X})
+      *v *= Bu;
+    for (double *v : {&F.p.h_disk, &F.p.w_disk, &F.p.rn, &F.p.rs, &F.p.wh, &F.p.z0,
+                      &F.p.rpc_X, &F.p.r0_X})
+      *v *= L;
+    // fractions of the circumference of each arm and the arm boundaries on
+    // the negative x axis (kpc), fixed in the model (breg_jf12.cc:49-58)
+    const double f[8] = {0.130, 0.165, 0.094, 0.122, 0.13, 0.118, 0.084, 0.156};
+    const double rc[8] = {5.1, 6.3, 7.1, 8.3, 9.8, 11.4, 12.7, 15.5};
+    const double bv[8] = {F.p.b_arm1, F.p.b_arm2, F.p.b_arm3, F.p.b_arm4,
+                          F.p.b_arm5, F.p.b_arm6, F.p.b_arm7, 0.};
+    double b8 = 0.;
+    for (int i = 0; i < 7; i++) b8 -= f[i] * bv[i] / f[7];
+    for (int i = 0; i < 7; i++) F.bv[i] = bv[i];
+    F.bv[7] = b8;
+    for (int i = 0; i < 8; i++) F.rc_b[i] = rc[i] * cgs::kpc * L;
+    const double inc = 11.5;  // degrees
+    F.cot_inc = 1 / std::tan(cgs::pi / 180. * (90 - inc));
+    F.sin_inc = std::sin(cgs::pi / 180. * inc);
+    F.cos_inc = std::cos(cgs::pi / 180. * inc);
+    F.tan_x = std::tan(m.jf12.Xtheta);
+    F.r_max = 20 * cgs::kpc * L;
+    F.rho_gc = 1. * cgs::kpc * L;
+    F.r_min = 5. * cgs::kpc * L;
+    F.r_cent = 3. * cgs::kpc * L;
+    F.tiny = 1.e-12 * Bu;
+  }
+  // TEreg_ymw16 (tereg_ymw16.cc:233-240, 305-307)
+  {
+    Ymw16Dev &Y = d.ymw16;
+    Y.p = m.ymw16;
+    hxg_tereg_ymw16_t &q = Y.p;
+    for (double *v : {&q.r_warp, &q.r0, &q.t1_ad, &q.t1_bd, &q.t1_h1, &q.t2_a2, &q.t2_b2,
+                      &q.t3_b2s, &q.t3_aa, &q.t4_agc, &q.t4_hgc, &q.t5_wgn, &q.t5_agn,
+                      &q.t6_wlb1, &q.t6_hlb1, &q.t6_wlb2, &q.t6_hlb2, &q.t7_rli, &q.t7_wli})
+      *v *= L;
+    for (int k = 0; k < 5; ++k) {
+      q.t3_warm[k] *= L;
+      q.t3_rmin[k] *= L;
+    }
+    Y.pc = cgs::pc * L;
+    Y.kpc = cgs::kpc * L;
+    const double lc = 264. * cgs::rad, bc = -4. * cgs::rad, dc = 450. * cgs::pc * L;
+    Y.gum_xc = dc * std::cos(bc) * std::sin(lc);
+    Y.gum_yc = q.r0 - dc * std::cos(bc) * std::cos(lc);
+    Y.gum_zc = dc * std::sin(bc);
+    Y.cos_li = std::cos((m.ymw16.t7_thetali) * cgs::rad);
+    Y.sin_li = std::sin((m.ymw16.t7_thetali) * cgs::rad);
+  }
   return d;
 }
 

@@ -19,6 +19,7 @@ constexpr double pi = 3.141592653589793238462643383279502884197;
 constexpr double halfpi = 1.570796326794896619231321691639751442099;
 constexpr double twothirds = 0.666666666666666666666666666666666666667;
 constexpr double twopi = 6.283185307179586476925286766559005768394;
+constexpr double rad = (pi / 180.);
 constexpr double erg = 1., cm = 1., sec = 1., Kelvin = 1.;
 constexpr double m = (1.e2 * cm);
 constexpr double pc = (3.0856775806e+18 * cm);

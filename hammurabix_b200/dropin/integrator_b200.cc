@@ -117,6 +117,43 @@ hxg_models_t map_models(DeviceState &s, const Breg *breg, const Brnd *,
       m.breg = HXG_BREG_HELIX;
       m.helix = {par->breg_helix.bx, par->breg_helix.by, par->breg_helix.bz,
                  par->breg_helix.r_min, par->breg_helix.r_max};
+    } else if (dynamic_cast<const Breg_jaffe *>(breg)) {
+      m.breg = HXG_BREG_JAFFE;
+      const auto &j = par->breg_jaffe;
+      auto &d = m.jaffe;
+      d.quadruple = j.quadruple;
+      d.bss = j.bss;
+      d.ring = j.ring;
+      d.bar = j.bar;
+      d.arm_num = (uint32_t)std::min<std::size_t>(j.arm_num, 8);
+      d.disk_amp = j.disk_amp;
+      d.disk_z0 = j.disk_z0;
+      d.halo_amp = j.halo_amp;
+      d.halo_z0 = j.halo_z0;
+      d.r_inner = j.r_inner;
+      d.r_scale = j.r_scale;
+      d.r_peak = j.r_peak;
+      d.ring_amp = j.ring_amp;
+      d.bar_amp = j.bar_amp;
+      d.ring_r = j.ring_r;
+      d.bar_a = j.bar_a;
+      d.bar_b = j.bar_b;
+      d.bar_phi0 = j.bar_phi0;
+      for (std::size_t k = 0; k < j.arm_amp.size() && k < 8; ++k) d.arm_amp[k] = j.arm_amp[k];
+      for (std::size_t k = 0; k < j.arm_phi0.size() && k < 8; ++k) d.arm_phi0[k] = j.arm_phi0[k];
+      d.arm_pitch = j.arm_pitch;
+      d.arm_r0 = j.arm_r0;
+      d.arm_z0 = j.arm_z0;
+      d.comp_r = j.comp_r;
+      d.comp_c = j.comp_c;
+      d.comp_d = j.comp_d;
+      d.comp_p = j.comp_p;
+    } else if (dynamic_cast<const Breg_jf12 *>(breg)) {
+      m.breg = HXG_BREG_JF12;
+      const auto &j = par->breg_jf12;
+      m.jf12 = {j.b_arm1, j.b_arm2, j.b_arm3, j.b_arm4, j.b_arm5, j.b_arm6, j.b_arm7,
+                j.b_ring, j.h_disk, j.w_disk, j.Bn, j.Bs, j.rn, j.rs, j.wh, j.z0,
+                j.B0_X, j.Xtheta, j.rpc_X, j.r0_X};
     } else if (typeid(*breg) == typeid(Breg)) {
       m.breg = HXG_BREG_NONE;
     } else {

@@ -96,6 +96,40 @@ def case_models():
     return out
 
 
+def obs_models_ext():
+    """Pass of the large-model cases: 3 shells (Nside 8/16/32) to 20 kpc at
+    0.05 kpc, DM + FD + sync at 1.4 GHz, output Nside 32."""
+    return [W.make_obs([8, 16, 32], 20.0, 0.05, freq_ghz=1.4)]
+
+
+def case_models_ext(blocks):
+    """Breg_jaffe with its molecular ring and with its elliptical bar, and
+    Breg_jf12, each with TEreg_ymw16 or the exponential disk; `blocks` holds
+    the jaffe / jf12 / ymw16 parameter blocks (the reference template's
+    values; the fixtures store the full model block of every case)."""
+    out = []
+    def mk(breg, tereg, cre):
+        m = W.spiral_models()
+        m.breg, m.tereg, m.cre = breg, tereg, cre
+        m.jaffe = blocks["jaffe"]
+        m.jf12 = blocks["jf12"]
+        m.ymw16 = blocks["ymw16"]
+        m.cre_unif.alpha = 3.0
+        m.cre_unif.r0 = 3.0 * U.kpc
+        m.cre_unif.E0 = 20.6 * U.GeV
+        m.cre_unif.j0 = 0.0217
+        return m
+    m = mk(abi.HXG_BREG_JAFFE, abi.HXG_TEREG_YMW16, abi.HXG_CRE_ANA)
+    m.jaffe.ring, m.jaffe.bar = 1, 0
+    out.append(("jaffe_ring_ymw16", m))
+    m = mk(abi.HXG_BREG_JAFFE, abi.HXG_TEREG_EXPDISK, abi.HXG_CRE_ANA)
+    m.jaffe.ring, m.jaffe.bar = 0, 1
+    out.append(("jaffe_bar_expdisk", m))
+    out.append(("jf12_ymw16", mk(abi.HXG_BREG_JF12, abi.HXG_TEREG_YMW16, abi.HXG_CRE_UNIF)))
+    out.append(("spiral_ymw16", mk(abi.HXG_BREG_SPIRAL, abi.HXG_TEREG_YMW16, abi.HXG_CRE_ANA)))
+    return out
+
+
 def case_dm_only():
     """DM-only pass (no FD, no sync) with two grid geometries."""
     o = W.make_obs([8, 16], 25.0, 0.05, freq_ghz=None, do_fd=False)

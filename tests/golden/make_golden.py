@@ -11,6 +11,11 @@ that holds the hammurabiX source tree; the outputs are committed).
 3. ref_maps.npz -- full DM / FD / I / Q / U maps computed by the reference
    integrator itself (compiled from its sources by oracle/Makefile) on the
    small cases of tests/cases.py, plus the FP32 field grids those cases use.
+4. ref_models_ext.npz -- the same for the Breg_jaffe (ring and bar),
+   Breg_jf12 and TEreg_ymw16 models with the parameter values of the
+   reference's templates/params_template.xml (parsed by
+   hammurabix_b200.param with Param's unit conversions); the hxg_models_t
+   block of each case is stored beside its maps.
 
 Usage: python tests/golden/make_golden.py [hammurabiX source dir]
 """
@@ -74,9 +79,43 @@ def reference_maps():
     np.savez_compressed(os.path.join(HERE, "ref_maps.npz"), **out)
 
 
+def _template_blocks(src):
+    """jaffe / jf12 / ymw16 parameter blocks of the reference's template."""
+    import tempfile
+    import xml.etree.ElementTree as ET
+    from hammurabix_b200.param import Param
+    tree = ET.parse(os.path.join(src, "templates", "params_template.xml"))
+    root = tree.getroot()
+    blocks = {}
+    for btype, tetype in (("jaffe", "ymw16"), ("jf12", "ymw16")):
+        root.find("magneticfield").find("regular").set("type", btype)
+        root.find("thermalelectron").find("regular").set("type", tetype)
+        with tempfile.NamedTemporaryFile("w", suffix=".xml", delete=False) as f:
+            tree.write(f, encoding="unicode")
+        try:
+            m = Param(f.name).models
+        finally:
+            os.unlink(f.name)
+        blocks[btype] = getattr(m, btype)
+        blocks["ymw16"] = m.ymw16
+    return blocks
+
+
+def reference_models_ext(src):
+    ref = pyoracle.Reference()
+    blocks = _template_blocks(src)
+    out = {}
+    for name, m in cases.case_models_ext(blocks):
+        passes = cases.obs_models_ext()
+        _run(ref, passes, m, None, None, name, out)
+        out[f"{name}/models"] = np.frombuffer(bytes(m), dtype=np.uint8).copy()
+    np.savez_compressed(os.path.join(HERE, "ref_models_ext.npz"), **out)
+
+
 if __name__ == "__main__":
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     reference_fixtures(src)
     reference_maps()
+    reference_models_ext(src)
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))
