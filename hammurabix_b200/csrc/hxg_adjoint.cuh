@@ -64,7 +64,7 @@ __device__ __forceinline__ void flush_cell(double *grad_rec, long long key,
       }
 }
 
-template <int NG>
+template <int NG, bool kExt>
 __global__ void __launch_bounds__(256)
 shell_fp64_adjoint_kernel(const AdjointLaunch A) {
   const ShellLaunch &P = A.F;
@@ -177,8 +177,8 @@ shell_fp64_adjoint_kernel(const AdjointLaunch A) {
           pz > P.gc_z_max)
         continue;
       const double p3[3] = {px, py, pz};
-      const V3<double> Breg = breg_model<double>(M, px, py, pz, p3);
-      const double tereg = tereg_model<double>(M, px, py, pz, p3);
+      const V3<double> Breg = breg_model_x<kExt>(M, P.ext, px, py, pz, p3);
+      const double tereg = tereg_model_x<kExt>(M, P.ext, px, py, pz, p3);
       double b3[3] = {Breg.x, Breg.y, Breg.z};
       double te = tereg;
       bool in_grid = false;
@@ -281,11 +281,9 @@ shell_fp64_adjoint_kernel(const AdjointLaunch A) {
         const double r = sqrt(px * px + py * py);
         const double gdotb = gbx * Breg.x + gby * Breg.y;
         gp[0] += gdotb / M.sp_b0;
-        const double cos_p = px / r, sin_p = py / r;
-        const double amp = M.sp_b0 * exp(-(r - M.sp_rsun) / M.sp_rs) *
-                           exp(-fabs(pz) / M.sp_hs);
-        gp[1] += amp * (gbx * (M.sp_cos * cos_p + M.sp_sin * sin_p) +
-                        gby * (M.sp_cos * sin_p - M.sp_sin * cos_p));
+        // B = amp (sin(pitch - phi), cos(pitch - phi)), so dB/dpitch is B
+        // turned by -90 degrees: (B_y, -B_x)
+        gp[1] += gbx * Breg.y - gby * Breg.x;
         gp[2] += gdotb * (r - M.sp_rsun) / (M.sp_rs * M.sp_rs);
         gp[3] += gdotb * fabs(pz) / (M.sp_hs * M.sp_hs);
       }

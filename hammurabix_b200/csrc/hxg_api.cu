@@ -81,6 +81,7 @@ struct hxg_handle {
   std::vector<DevBuf> ck, ck_inner;
   std::vector<int> ck_chunks;
   DevBuf grad_rec, grad_par, g_shell[5], g_fdmap;
+  DevBuf ext;  // ExtModels block of the current launches
 };
 
 namespace {
@@ -362,10 +363,21 @@ DevModels dev_models(const hxg_models_t &m, const double obs[3], double L,
     d.cre_unif_r0 = m.cre_unif.r0 * L;
   }
   d.cre_R0 = rsun * L;
+  return d;
+}
+
+// Models whose blocks live in ExtModels (separate kernel instantiations).
+bool uses_ext(const hxg_models_t &m) {
+  return m.breg == HXG_BREG_JAFFE || m.breg == HXG_BREG_JF12 || m.tereg == HXG_TEREG_YMW16;
+}
+
+// Jaffe / JF12 / YMW16 blocks in the working units of the form.
+void ext_models(const hxg_models_t &m, double L, double Bu, ExtModels &x) {
+  std::memset(&x, 0, sizeof(x));
   // Breg_jaffe: the Param block in working units and its parameter-only
   // constants (breg_jaffe.cc:14-17, 42-46, 107-108, 183-187)
   {
-    JaffeDev &J = d.jaffe;
+    JaffeDev &J = x.jaffe;
     J.p = m.jaffe;
     for (double *v : {&J.p.disk_amp, &J.p.halo_amp, &J.p.ring_amp, &J.p.bar_amp}) *v *= Bu;
     for (int k = 0; k < 8; ++k) J.p.arm_amp[k] *= Bu;
@@ -384,7 +396,7 @@ DevModels dev_models(const hxg_models_t &m, const double obs[3], double L,
   }
   // Breg_jf12 (breg_jf12.cc:10-62, 96-104)
   {
-    Jf12Dev &F = d.jf12;
+    Jf12Dev &F = x.jf12;
     F.p = m.jf12;
     for (double *v : {&F.p.b_arm1, &F.p.b_arm2, &F.p.b_arm3, &F.p.b_arm4, &F.p.b_arm5,
                       &F.p.b_arm6, &F.p.b_arm7, &F.p.b_ring, &F.p.Bn, &F.p.Bs, &F.p.B0_X})
@@ -416,7 +428,7 @@ DevModels dev_models(const hxg_models_t &m, const double obs[3], double L,
   }
   // TEreg_ymw16 (tereg_ymw16.cc:233-240, 305-307)
   {
-    Ymw16Dev &Y = d.ymw16;
+    Ymw16Dev &Y = x.ymw16;
     Y.p = m.ymw16;
     hxg_tereg_ymw16_t &q = Y.p;
     for (double *v : {&q.r_warp, &q.r0, &q.t1_ad, &q.t1_bd, &q.t1_h1, &q.t2_a2, &q.t2_b2,
@@ -436,7 +448,22 @@ DevModels dev_models(const hxg_models_t &m, const double obs[3], double L,
     Y.cos_li = std::cos((m.ymw16.t7_thetali) * cgs::rad);
     Y.sin_li = std::sin((m.ymw16.t7_thetali) * cgs::rad);
   }
-  return d;
+}
+
+// Upload the handle's ExtModels block for models m; *dev = its device
+// address, or null when m uses none of the three models.
+int upload_ext(hxg_handle *h, const hxg_models_t &m, const ExtModels **dev) {
+  *dev = nullptr;
+  if (!uses_ext(m)) return HXG_OK;
+  const bool fp32 = h->precision == HXG_FP32C;
+  ExtModels x;
+  ext_models(m, fp32 ? 1.0 / cgs::kpc : 1.0, fp32 ? 1.0 / cgs::fp32_bunit : 1.0, x);
+  int st = ensure(h, h->ext, sizeof(ExtModels));
+  if (st != HXG_OK) return st;
+  // pageable source: the call returns once the bytes are staged
+  HXG_CK(cudaMemcpyAsync(h->ext.p, &x, sizeof(x), cudaMemcpyHostToDevice, h->stream));
+  *dev = static_cast<const ExtModels *>(h->ext.p);
+  return HXG_OK;
 }
 
 int choose_chunks(const hxg_handle *h, uint64_t npix, uint64_t step) {
@@ -658,7 +685,8 @@ int noalloc_shell_launch(const hxg_obs_t *o, const hxg_models_t *m,
 
 bool noalloc_models_supported(const hxg_models_t *m) {
   std::string why;
-  return models_supported(*m, &why);
+  // the Jaffe / JF12 / YMW16 blocks would need a device allocation
+  return models_supported(*m, &why) && !uses_ext(*m);
 }
 
 bool noalloc_obs_valid(const hxg_obs_t *o) {
@@ -817,10 +845,13 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
     HXG_CK(cudaMemsetAsync(d_qs, 0, b, h->stream));
     HXG_CK(cudaMemsetAsync(d_us, 0, b, h->stream));
   }
+  const ExtModels *ext_dev = nullptr;
+  if ((st = upload_ext(h, h->models, &ext_dev)) != HXG_OK) return st;
   for (uint32_t s = 0; s < o->total_shell; ++s) {
     ShellLaunch P;
     uint64_t step;
     if ((st = build_launch(h, h->models, *o, s, P, step)) != HXG_OK) return st;
+    P.ext = ext_dev;
     // inner-shell Faraday depth: the accumulated FD output map when it is
     // requested, otherwise an all-zero map (integrator.cc:78-86, 130-132)
     P.fdmap = o->do_fd ? d_fd : nullptr;
@@ -948,10 +979,13 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
       return st;
   double *gs[5];
   for (int k = 0; k < 5; ++k) gs[k] = static_cast<double *>(h->g_shell[k].p);
+  const ExtModels *ext_dev = nullptr;
+  if ((st = upload_ext(h, h->models, &ext_dev)) != HXG_OK) return st;
   for (int s = (int)o->total_shell - 1; s >= 0; --s) {
     ShellLaunch F;
     uint64_t step;
     if ((st = build_launch(h, h->models, *o, (uint32_t)s, F, step)) != HXG_OK) return st;
+    F.ext = ext_dev;
     const int ns = (int)o->nside_shell[s];
     const uint64_t npix = npix_of((uint32_t)ns);
     for (int k = 0; k < 5; ++k)
@@ -1287,6 +1321,8 @@ struct hxg_batch {
   std::vector<size_t> tmp_off;  // per entry, doubles into tmp
   std::vector<size_t> tmp_n;    // per entry, doubles per map
   DevBuf tmp, zeros, zblocks, counters;
+  DevBuf ext;               // ExtModels per entry (entries that use them)
+  bool ext_any = false;
   std::vector<DevBuf> plans, tiles, merges, mblocks;
   std::vector<int> nplans, nmerge;
   std::vector<unsigned long long> merge_blocks;
@@ -1345,6 +1381,7 @@ int batch_tables(hxg_batch *b, int lanes, int grain) {
       L.fdmap = o.do_fd ? E.d_fd : nullptr;
       L.nside_fdmap = o.do_fd ? (int)o.nside_fd : 0;
       L.mask = nullptr;
+      L.ext = uses_ext(E.models) ? static_cast<const ExtModels *>(b->ext.p) + i : nullptr;
       double *t = tmp + b->tmp_off[i];
       for (int k = 0; k < 5; ++k) L.out[k] = t + k * b->tmp_n[i];
       int C = std::min(lanes, 32);
@@ -1404,7 +1441,8 @@ int batch_capture(hxg_batch *b) {
     B.nplans = b->nplans[l];
     B.grain = b->grain;
     B.counter = ctr + l;
-    if (B.nplans > 0) e = hxg::launch_batch_level(s, b->fp32, b->ngroups, B, b->level_blocks);
+    if (B.nplans > 0)
+      e = hxg::launch_batch_level(s, b->fp32, b->ngroups, b->ext_any, B, b->level_blocks);
     if (e != cudaSuccess) break;
     e = hxg::launch_batch_merge(s, static_cast<const MergeJob *>(b->merges[l].p),
                                 static_cast<const unsigned long long *>(b->mblocks[l].p),
@@ -1446,7 +1484,7 @@ int batch_time(hxg_batch *b, double *ms) {
 
 void batch_free(hxg_batch *b) {
   batch_drop_graph(b);
-  DevBuf *bufs[] = {&b->tmp, &b->zeros, &b->zblocks, &b->counters};
+  DevBuf *bufs[] = {&b->tmp, &b->zeros, &b->zblocks, &b->counters, &b->ext};
   for (DevBuf *d : bufs)
     if (d->p) cudaFree(d->p);
   for (auto *v : {&b->plans, &b->tiles, &b->merges, &b->mblocks})
@@ -1529,8 +1567,18 @@ int hxg_batch_create(hxg_handle *h, int n, const hxg_batch_entry_t *entries,
     return bail(st);
   if ((st = upload_vec(h, b->zeros, zj)) != HXG_OK) return bail(st);
   if ((st = upload_vec(h, b->zblocks, z0)) != HXG_OK) return bail(st);
+  {
+    std::vector<ExtModels> ext(b->e.size());
+    for (size_t i = 0; i < b->e.size(); ++i) {
+      if (!uses_ext(b->e[i].models)) continue;
+      b->ext_any = true;
+      ext_models(b->e[i].models, b->fp32 ? 1.0 / cgs::kpc : 1.0,
+                 b->fp32 ? 1.0 / cgs::fp32_bunit : 1.0, ext[i]);
+    }
+    if (b->ext_any && (st = upload_vec(h, b->ext, ext)) != HXG_OK) return bail(st);
+  }
   int per_sm = 0;
-  cudaError_t ce = hxg::batch_level_occupancy(b->fp32, b->ngroups, &per_sm);
+  cudaError_t ce = hxg::batch_level_occupancy(b->fp32, b->ngroups, b->ext_any, &per_sm);
   if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "occupancy"));
   b->level_blocks = (unsigned)std::max(1, per_sm) * (unsigned)h->sm_count;
   // launch shapes: lanes per pixel x tiles per work fetch

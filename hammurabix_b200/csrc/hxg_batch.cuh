@@ -23,7 +23,7 @@ struct BatchLevel {
   unsigned long long *counter;
 };
 
-template <int NG, bool kFp32>
+template <int NG, bool kFp32, bool kExt>
 __device__ __forceinline__ void batch_level_body(const BatchLevel &B) {
   const int lane = threadIdx.x & 31;
   const unsigned long long total = B.tile_start[B.nplans];
@@ -45,25 +45,25 @@ __device__ __forceinline__ void batch_level_body(const BatchLevel &B) {
       const ShellLaunch &P = B.plans[k];
       const long long gw = (long long)(t - B.tile_start[k]);
       if (kFp32)
-        fp32c_tile<NG>(P, gw, lane);
+        fp32c_tile<NG, kExt>(P, gw, lane);
       else
-        fp64_tile<NG, false>(P, gw, lane);
+        fp64_tile<NG, false, kExt>(P, gw, lane);
     }
   }
 }
 
 // The launch blocks are read from global memory, which needs more live
 // registers than the single-launch kernel: 2 resident blocks per SM.
-template <int NG>
+template <int NG, bool kExt>
 __global__ void __launch_bounds__(256, 2)
 batch_fp32c_kernel(const BatchLevel B) {
-  batch_level_body<NG, true>(B);
+  batch_level_body<NG, true, kExt>(B);
 }
 
-template <int NG>
+template <int NG, bool kExt>
 __global__ void __launch_bounds__(256)
 batch_fp64_kernel(const BatchLevel B) {
-  batch_level_body<NG, false>(B);
+  batch_level_body<NG, false, kExt>(B);
 }
 
 // Map merges of one level: job j adds nmaps shell maps at nside_src into

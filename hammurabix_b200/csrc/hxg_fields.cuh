@@ -42,10 +42,6 @@ struct DevModels {
   double tex_n0, tex_rs, tex_hs;
   // CRE_ana / CRE_unif (source/field/cre/cre_ana.cc, cre_unif.cc)
   double cre_alpha, cre_beta, cre_theta, cre_r0, cre_z0, cre_R0, cre_unif_r0;
-  // Breg_jaffe, Breg_jf12, TEreg_ymw16 (hxg_models_ext.cuh)
-  JaffeDev jaffe;
-  Jf12Dev jf12;
-  Ymw16Dev ymw16;
 };
 
 template <typename T>
@@ -123,19 +119,6 @@ __device__ __forceinline__ V3<T> breg_model(const DevModels &m, T x, T y,
       }
       return b;
     }
-    case kBregJaffe:
-    case kBregJf12:
-      if constexpr (sizeof(T) == 8) {
-        double bb[3];
-        if (m.breg == kBregJaffe)
-          breg_jaffe(m.jaffe, x, y, z, bb);
-        else
-          breg_jf12(m.jf12, x, y, z, bb);
-        b.x = bb[0];
-        b.y = bb[1];
-        b.z = bb[2];
-      }
-      return b;
     case kBregSpiral: {
       const T r = sqrt(x * x + y * y);
       if (outside_annulus<T>(r, p, m.kpc, 3., 20.)) return b;
@@ -163,12 +146,34 @@ __device__ __forceinline__ T tereg_model(const DevModels &m, T x, T y, T z,
       const T r = sqrt(x * x + y * y);
       return T(m.tex_n0) * exp(-r / T(m.tex_rs)) * exp(-fabs(z) / T(m.tex_hs));
     }
-    case kTeregYmw16:
-      if constexpr (sizeof(T) == 8) return tereg_ymw16(m.ymw16, x, y, z);
-      return T(0);
     default:
       return T(0);
   }
+}
+
+// Regular B and n_e including the models of hxg_models_ext.cuh (FP64).
+// kExt = false instantiations compile to breg_model / tereg_model alone.
+template <bool kExt>
+__device__ __forceinline__ V3<double> breg_model_x(const DevModels &m, const ExtModels *ext,
+                                                   double x, double y, double z,
+                                                   const double p[3]) {
+  if (kExt && (m.breg == kBregJaffe || m.breg == kBregJf12)) {
+    double bb[3];
+    if (m.breg == kBregJaffe)
+      breg_jaffe(ext->jaffe, x, y, z, bb);
+    else
+      breg_jf12(ext->jf12, x, y, z, bb);
+    return V3<double>{bb[0], bb[1], bb[2]};
+  }
+  return breg_model<double>(m, x, y, z, p);
+}
+
+template <bool kExt>
+__device__ __forceinline__ double tereg_model_x(const DevModels &m, const ExtModels *ext,
+                                                double x, double y, double z,
+                                                const double p[3]) {
+  if (kExt && m.tereg == kTeregYmw16) return tereg_ymw16(ext->ymw16, x, y, z);
+  return tereg_model<double>(m, x, y, z, p);
 }
 
 // ---- CRE spectral index and spatial profile (cre_ana.cc:11-37,

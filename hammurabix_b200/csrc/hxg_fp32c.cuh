@@ -120,7 +120,7 @@ __device__ __forceinline__ double rsqrt_fd(double t) {
 
 // Warp gw of shell launch P (32/C pixels, C lanes each).  All 32 lanes of
 // the warp call it with the same gw.
-template <int NG>
+template <int NG, bool kExt>
 __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw,
                                            int lane) {
   const int C = P.chunks;
@@ -223,13 +223,13 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw,
         if (fast_t) te_d = F.ex_n0 * exp_fd(-fma(r, F.ex_irn, fabs(pz) * F.ex_ihn));
       }
       if (slow_b) {
-        const V3<double> Br = breg_model<double>(M, px, py, pz, p3);
+        const V3<double> Br = breg_model_x<kExt>(M, P.ext, px, py, pz, p3);
         bp_d = fma(Br.x, ux, fma(Br.y, uy, Br.z * uz));
         bxr = float(Br.x);
         byr = float(Br.y);
         bzr = float(Br.z);
       }
-      if (slow_t) te_d = tereg_model<double>(M, px, py, pz, p3);
+      if (slow_t) te_d = tereg_model_x<kExt>(M, P.ext, px, py, pz, p3);
       float bg[4] = {0.f, 0.f, 0.f, 0.f};
       if (NG == 1) {
         const DevGridGroup &G = P.groups[0];
@@ -349,11 +349,11 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw,
   }
 }
 
-template <int NG>
+template <int NG, bool kExt>
 __global__ void __launch_bounds__(256, HXG_FP32C_MIN_BLOCKS)
 shell_fp32c_kernel(const ShellLaunch P) {
-  fp32c_tile<NG>(P, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
-                 threadIdx.x & 31);
+  fp32c_tile<NG, kExt>(P, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                       threadIdx.x & 31);
 }
 
 }  // namespace hxg

@@ -64,6 +64,7 @@ struct ShellLaunch {
   double *ck;
   double *ck_inner;
   FastModels fast;  // FP32C only
+  const ExtModels *ext;  // Jaffe / JF12 / YMW16 blocks (device), or null
 };
 
 // Sample window [lo, hi) of one ray: the samples that can pass the
@@ -175,7 +176,7 @@ __device__ __forceinline__ void ipa2(T xv, T yv, T &c2, T &s2) {
 // ===================================================================
 // Warp gw of shell launch P (32/C pixels, C lanes each).  All 32 lanes of
 // the warp call it with the same gw.
-template <int NG, bool kCache>
+template <int NG, bool kCache, bool kExt>
 __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
                                           int lane) {
   const int C = P.chunks;
@@ -226,8 +227,8 @@ __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
           pz > P.gc_z_max)
         continue;
       const double p3[3] = {px, py, pz};
-      V3<double> B = breg_model<double>(M, px, py, pz, p3);
-      double te = tereg_model<double>(M, px, py, pz, p3);
+      V3<double> B = breg_model_x<kExt>(M, P.ext, px, py, pz, p3);
+      double te = tereg_model_x<kExt>(M, P.ext, px, py, pz, p3);
       if (NG > 0) {
         double b3[3] = {B.x, B.y, B.z};
 #pragma unroll 1
@@ -305,11 +306,11 @@ __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
   }
 }
 
-template <int NG, bool kCache>
+template <int NG, bool kCache, bool kExt>
 __global__ void __launch_bounds__(256)
 shell_fp64_kernel(const ShellLaunch P) {
-  fp64_tile<NG, kCache>(P, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
-                        threadIdx.x & 31);
+  fp64_tile<NG, kCache, kExt>(P, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                              threadIdx.x & 31);
 }
 
 }  // namespace hxg

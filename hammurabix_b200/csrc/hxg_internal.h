@@ -41,9 +41,9 @@ cudaError_t launch_accumulate_transpose(cudaStream_t s, int nside_out,
                                         double *g_shell, double scale);
 cudaError_t launch_adjoint(cudaStream_t s, const AdjointLaunch &A,
                            unsigned blocks, unsigned threads);
-cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups,
+cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups, bool ext,
                                const BatchLevel &B, unsigned blocks);
-cudaError_t batch_level_occupancy(bool fp32, int ngroups, int *blocks_per_sm);
+cudaError_t batch_level_occupancy(bool fp32, int ngroups, bool ext, int *blocks_per_sm);
 cudaError_t launch_batch_merge(cudaStream_t s, const MergeJob *jobs,
                                const unsigned long long *block0, int njobs,
                                unsigned long long nblocks);

@@ -2,6 +2,8 @@
 // packing, and the instantiations of the shell-integration kernels.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "hxg_adjoint.cuh"
 #include "hxg_batch.cuh"
 #include "hxg_fp32c.cuh"
@@ -278,57 +280,55 @@ cudaError_t launch_pack(cudaStream_t s, bool fp32, uint64_t n, void *rec,
   return cudaGetLastError();
 }
 
+// The kernels are instantiated per grid-group count (0, 1, up to
+// kMaxGroups) and per use of the Jaffe / JF12 / YMW16 blocks.
+template <typename F>
+static cudaError_t by_shape(int ngroups, bool ext, F &&f) {
+  const auto g = [&](auto ng) {
+    if (ext)
+      f(ng, std::true_type{});
+    else
+      f(ng, std::false_type{});
+  };
+  if (ngroups == 0)
+    g(std::integral_constant<int, 0>{});
+  else if (ngroups == 1)
+    g(std::integral_constant<int, 1>{});
+  else
+    g(std::integral_constant<int, 4>{});
+  return cudaGetLastError();
+}
+
 cudaError_t launch_shell(cudaStream_t s, bool fp32, const ShellLaunch &P,
                          unsigned blocks, unsigned threads) {
-  const int ng = P.ngroups;
-  if (fp32) {
-    if (ng == 0)
-      shell_fp32c_kernel<0><<<blocks, threads, 0, s>>>(P);
-    else if (ng == 1)
-      shell_fp32c_kernel<1><<<blocks, threads, 0, s>>>(P);
+  return by_shape(P.ngroups, P.ext != nullptr, [&](auto ng, auto ext) {
+    if (fp32)
+      shell_fp32c_kernel<decltype(ng)::value, decltype(ext)::value>
+          <<<blocks, threads, 0, s>>>(P);
     else
-      shell_fp32c_kernel<4><<<blocks, threads, 0, s>>>(P);
-  } else {
-    if (ng == 0)
-      shell_fp64_kernel<0, false><<<blocks, threads, 0, s>>>(P);
-    else if (ng == 1)
-      shell_fp64_kernel<1, false><<<blocks, threads, 0, s>>>(P);
-    else
-      shell_fp64_kernel<4, false><<<blocks, threads, 0, s>>>(P);
-  }
-  return cudaGetLastError();
+      shell_fp64_kernel<decltype(ng)::value, false, decltype(ext)::value>
+          <<<blocks, threads, 0, s>>>(P);
+  });
 }
 
-cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups,
+cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups, bool ext,
                                const BatchLevel &B, unsigned blocks) {
-  if (fp32) {
-    if (ngroups == 0)
-      batch_fp32c_kernel<0><<<blocks, 256, 0, s>>>(B);
-    else if (ngroups == 1)
-      batch_fp32c_kernel<1><<<blocks, 256, 0, s>>>(B);
+  return by_shape(ngroups, ext, [&](auto ng, auto ex) {
+    if (fp32)
+      batch_fp32c_kernel<decltype(ng)::value, decltype(ex)::value><<<blocks, 256, 0, s>>>(B);
     else
-      batch_fp32c_kernel<4><<<blocks, 256, 0, s>>>(B);
-  } else {
-    if (ngroups == 0)
-      batch_fp64_kernel<0><<<blocks, 256, 0, s>>>(B);
-    else if (ngroups == 1)
-      batch_fp64_kernel<1><<<blocks, 256, 0, s>>>(B);
-    else
-      batch_fp64_kernel<4><<<blocks, 256, 0, s>>>(B);
-  }
-  return cudaGetLastError();
+      batch_fp64_kernel<decltype(ng)::value, decltype(ex)::value><<<blocks, 256, 0, s>>>(B);
+  });
 }
 
-cudaError_t batch_level_occupancy(bool fp32, int ngroups, int *blocks_per_sm) {
-  const void *f;
-  if (fp32)
-    f = ngroups == 0 ? (const void *)batch_fp32c_kernel<0>
-        : ngroups == 1 ? (const void *)batch_fp32c_kernel<1>
-                       : (const void *)batch_fp32c_kernel<4>;
-  else
-    f = ngroups == 0 ? (const void *)batch_fp64_kernel<0>
-        : ngroups == 1 ? (const void *)batch_fp64_kernel<1>
-                       : (const void *)batch_fp64_kernel<4>;
+cudaError_t batch_level_occupancy(bool fp32, int ngroups, bool ext, int *blocks_per_sm) {
+  const void *f = nullptr;
+  by_shape(ngroups, ext, [&](auto ng, auto ex) {
+    if (fp32)
+      f = (const void *)batch_fp32c_kernel<decltype(ng)::value, decltype(ex)::value>;
+    else
+      f = (const void *)batch_fp64_kernel<decltype(ng)::value, decltype(ex)::value>;
+  });
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, 256, 0);
 }
 
@@ -359,10 +359,13 @@ cudaError_t launch_accumulate_transpose(cudaStream_t s, int nside_out,
 
 cudaError_t launch_adjoint(cudaStream_t s, const AdjointLaunch &A,
                            unsigned blocks, unsigned threads) {
+  const bool ext = A.F.ext != nullptr;
   if (A.F.ngroups == 0)
-    shell_fp64_adjoint_kernel<0><<<blocks, threads, 0, s>>>(A);
+    ext ? shell_fp64_adjoint_kernel<0, true><<<blocks, threads, 0, s>>>(A)
+        : shell_fp64_adjoint_kernel<0, false><<<blocks, threads, 0, s>>>(A);
   else
-    shell_fp64_adjoint_kernel<1><<<blocks, threads, 0, s>>>(A);
+    ext ? shell_fp64_adjoint_kernel<1, true><<<blocks, threads, 0, s>>>(A)
+        : shell_fp64_adjoint_kernel<1, false><<<blocks, threads, 0, s>>>(A);
   return cudaGetLastError();
 }
 

@@ -16,8 +16,6 @@
 
 namespace hxg {
 
-struct DevModels;
-
 // pow(1 / cosh(x), 2) as TEreg_ymw16 writes it
 __device__ __forceinline__ double sech2(double x) {
   const double c = 1. / cosh(x);
@@ -397,5 +395,14 @@ static __device__ __noinline__ double tereg_ymw16(const Ymw16Dev &Y, double x, d
                        w_gum * ne_comp[5]) +
          (w_lb) * (ne_comp[6]);
 }
+
+// The three models' parameter blocks of one launch, in device memory (the
+// kernels that read them are separate instantiations, so the common path
+// carries neither their code nor their parameters).
+struct ExtModels {
+  JaffeDev jaffe;
+  Jf12Dev jf12;
+  Ymw16Dev ymw16;
+};
 
 }  // namespace hxg
