@@ -12,6 +12,7 @@
 #include <cstring>
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -82,6 +83,7 @@ struct hxg_handle {
   std::vector<int> ck_chunks;
   DevBuf grad_rec, grad_par, g_shell[5], g_fdmap;
   DevBuf ext;  // ExtModels block of the current launches
+  DevBuf cre_tab;  // synchrotron tables + CRE energy tables
 };
 
 namespace {
@@ -157,7 +159,8 @@ bool models_supported(const hxg_models_t &m, std::string *why) {
     *why = "random n_e model must be NONE or GRID";
     return false;
   }
-  if (m.cre != HXG_CRE_NONE && m.cre != HXG_CRE_ANA && m.cre != HXG_CRE_UNIF) {
+  if (m.cre != HXG_CRE_NONE && m.cre != HXG_CRE_ANA && m.cre != HXG_CRE_UNIF &&
+      m.cre != HXG_CRE_GRID) {
     *why = "CRE model not supported on the device";
     return false;
   }
@@ -368,8 +371,61 @@ DevModels dev_models(const hxg_models_t &m, const double obs[3], double L,
 
 // Models whose blocks live in ExtModels (separate kernel instantiations).
 bool uses_ext(const hxg_models_t &m) {
-  return m.breg == HXG_BREG_JAFFE || m.breg == HXG_BREG_JF12 || m.tereg == HXG_TEREG_YMW16;
+  return m.breg == HXG_BREG_JAFFE || m.breg == HXG_BREG_JF12 ||
+         m.tereg == HXG_TEREG_YMW16 || m.cre == HXG_CRE_GRID;
 }
+
+// ---- synchrotron functions for the CRE-grid emissivity ------------------
+// F(x) = x Int_x^inf K_{5/3}(t) dt and G(x) = x K_{2/3}(x) (the functions
+// gsl_sf_synchrotron_1/2 evaluate, integrator.cc:320, 396), tabulated as
+// ln(F/x^(1/3)), ln(G/x^(1/3)) on 32768 points of u = ln x in
+// [ln 1e-24, ln 128].
+// The integral runs down from x = 128 by 10-point Gauss-Legendre panels
+// between consecutive table points (Int_128^inf K_{5/3} below 1e-54).
+constexpr int kSynchroN = 32768;
+constexpr double kSynchroU0 = -55.262042231857095;  // ln 1e-24
+constexpr double kSynchroU1 = 4.852030263919617;    // ln 128
+
+const std::vector<double> &synchro_tables() {
+  static std::vector<double> tab;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    const double gx[10] = {-0.9739065285171717, -0.8650633666889845, -0.6794095682990244,
+                           -0.4333953941292472, -0.1488743389816312, 0.1488743389816312,
+                           0.4333953941292472,  0.6794095682990244,  0.8650633666889845,
+                           0.9739065285171717};
+    const double gw[10] = {0.0666713443086881, 0.1494513491505806, 0.2190863625159820,
+                           0.2692667193099963, 0.2955242247147529, 0.2955242247147529,
+                           0.2692667193099963, 0.2190863625159820, 0.1494513491505806,
+                           0.0666713443086881};
+    const int n = kSynchroN;
+    const double du = (kSynchroU1 - kSynchroU0) / (n - 1);
+    tab.assign(2 * n, 0.);
+    // Int_{x_k}^{x_{k+1}} K_{5/3}(t) dt with t = e^u, dt = t du
+    double acc = 0.;
+    for (int k = n - 1; k >= 0; --k) {
+      const double u = kSynchroU0 + k * du;
+      const double x = std::exp(u);
+      if (k < n - 1) {
+        double seg = 0.;
+        for (int q = 0; q < 10; ++q) {
+          const double uq = u + 0.5 * du * (gx[q] + 1.);
+          const double t = std::exp(uq);
+          seg += gw[q] * std::cyl_bessel_k(5. / 3., t) * t;
+        }
+        acc += 0.5 * du * seg;
+      }
+      tab[k] = std::log(x * acc / std::cbrt(x));                          // ln F/x^(1/3)
+      tab[n + k] = std::log(x * std::cyl_bessel_k(2. / 3., x) / std::cbrt(x));  // ln G/x^(1/3)
+    }
+  });
+  return tab;
+}
+
+// Device copies of the CRE grid's energy tables and the synchrotron tables,
+// and the CreGridDev block in working units (L, Bu of the form).
+int cre_grid_block(hxg_handle *h, double L, double Bu, double freq, CreGridDev &c);
+
 
 // Jaffe / JF12 / YMW16 blocks in the working units of the form.
 void ext_models(const hxg_models_t &m, double L, double Bu, ExtModels &x) {
@@ -452,17 +508,69 @@ void ext_models(const hxg_models_t &m, double L, double Bu, ExtModels &x) {
 
 // Upload the handle's ExtModels block for models m; *dev = its device
 // address, or null when m uses none of the three models.
-int upload_ext(hxg_handle *h, const hxg_models_t &m, const ExtModels **dev) {
+int upload_ext(hxg_handle *h, const hxg_models_t &m, double freq, const ExtModels **dev) {
   *dev = nullptr;
   if (!uses_ext(m)) return HXG_OK;
   const bool fp32 = h->precision == HXG_FP32C;
   ExtModels x;
-  ext_models(m, fp32 ? 1.0 / cgs::kpc : 1.0, fp32 ? 1.0 / cgs::fp32_bunit : 1.0, x);
+  const double L = fp32 ? 1.0 / cgs::kpc : 1.0, Bu = fp32 ? 1.0 / cgs::fp32_bunit : 1.0;
+  ext_models(m, L, Bu, x);
+  if (m.cre == HXG_CRE_GRID) {
+    const int st = cre_grid_block(h, L, Bu, freq, x.cre);
+    if (st != HXG_OK) return st;
+  }
   int st = ensure(h, h->ext, sizeof(ExtModels));
   if (st != HXG_OK) return st;
   // pageable source: the call returns once the bytes are staged
   HXG_CK(cudaMemcpyAsync(h->ext.p, &x, sizeof(x), cudaMemcpyHostToDevice, h->stream));
   *dev = static_cast<const ExtModels *>(h->ext.p);
+  return HXG_OK;
+}
+
+int cre_grid_block(hxg_handle *h, double L, double Bu, double freq, CreGridDev &c) {
+  const Slot &S = h->slots[HXG_FIELD_CRE];
+  if (!S.present) return fail(h, HXG_ERR_STATE, "CRE grid model without an uploaded CRE grid");
+  const hxg_grid_desc_t &g = S.desc;
+  const int nE = (int)g.nE;
+  const std::vector<double> &tab = synchro_tables();
+  // device layout: tab_f | tab_g | inv_ke2[nE] | beta[nE] | dke[nE-1]
+  std::vector<double> host(tab);
+  std::vector<double> ke(nE);
+  for (int i = 0; i < nE; ++i) ke[i] = g.E_min * std::exp(i * g.E_fact);  // integrator.cc:300-304
+  for (int i = 0; i < nE; ++i) host.push_back(1. / (ke[i] * ke[i]));
+  for (int i = 0; i < nE; ++i) host.push_back(std::sqrt(1 - cgs::mec2 / ke[i]));
+  for (int i = 0; i + 1 < nE; ++i) host.push_back(std::fabs(ke[i + 1] - ke[i]));
+  int st = ensure(h, h->cre_tab, host.size() * sizeof(double));
+  if (st != HXG_OK) return st;
+  HXG_CK(cudaMemcpy(h->cre_tab.p, host.data(), host.size() * sizeof(double),
+                    cudaMemcpyHostToDevice));
+  const double *d = static_cast<const double *>(h->cre_tab.p);
+  c.flux = S.d[0];
+  c.nx = (int)g.nx;
+  c.ny = (int)g.ny;
+  c.nz = (int)g.nz;
+  c.nE = nE;
+  c.lo[0] = g.x_min * L;
+  c.lo[1] = g.y_min * L;
+  c.lo[2] = g.z_min * L;
+  c.hi[0] = g.x_max * L;
+  c.hi[1] = g.y_max * L;
+  c.hi[2] = g.z_max * L;
+  c.tab_f = d;
+  c.tab_g = d + kSynchroN;
+  c.inv_ke2 = d + 2 * kSynchroN;
+  c.beta = c.inv_ke2 + nE;
+  c.dke = c.beta + nE;
+  c.u0 = kSynchroU0;
+  c.inv_du = (kSynchroN - 1) / (kSynchroU1 - kSynchroU0);
+  c.ntab = kSynchroN;
+  // x_fact numerators and fore factor in the reference's order
+  // (integrator.cc:297-299, 319-325, 367-369, 382-385)
+  c.xnum_t = 4. * cgs::pi * freq * cgs::mec * cgs::mec2 * cgs::mec2;
+  c.xnum_p = (2. * cgs::mec * cgs::mec2 * cgs::mec2 * 2. * cgs::pi * freq);
+  c.fore_num = 1.73205081 * cgs::qe * cgs::qe * cgs::qe;
+  c.fore_den = cgs::mec2 * cgs::c_light * cgs::GeV * cgs::m * cgs::m * cgs::sec;
+  c.bunit = 1. / Bu;
   return HXG_OK;
 }
 
@@ -510,8 +618,13 @@ int build_launch(hxg_handle *h, const hxg_models_t &m, const hxg_obs_t &o,
     P.tc_b = 1.;
   }
   P.models = dev_models(m, o.observer, L, Bu);
+  // CRE grid: the emissivity is integrated per sample (cre_grid_j); the
+  // FP32C form scales it by 2^128 into FP32 range and k_t = k_p undo that
+  if (P.do_sync && m.cre == HXG_CRE_GRID) {
+    P.k_t = P.k_p = delta * P.i2bt * 0x1p-128;
+  }
   // analytic synchrotron emissivity constants (integrator.cc:332-346, 401-415)
-  if (P.do_sync) {
+  if (P.do_sync && m.cre != HXG_CRE_GRID) {
     const double E0 = m.cre == HXG_CRE_ANA ? m.cre_ana.E0 : m.cre_unif.E0;
     const double j0 = m.cre == HXG_CRE_ANA ? m.cre_ana.j0 : m.cre_unif.j0;
     const double gamma0 = E0 / cgs::mec2;
@@ -623,8 +736,8 @@ int upload_common(hxg_handle *h, int field, const hxg_grid_desc_t *g,
   if (!h) return HXG_ERR_INVALID;
   if (field < 0 || field > HXG_FIELD_CRE || !g)
     return fail(h, HXG_ERR_INVALID, "bad field slot %d", field);
-  if (field == HXG_FIELD_CRE)
-    return fail(h, HXG_ERR_UNSUPPORTED, "CRE grids are not supported on the device");
+  if (field == HXG_FIELD_CRE && (g->nE < 2 || !(g->E_fact > 0.) || !(g->E_min > 0.)))
+    return fail(h, HXG_ERR_INVALID, "CRE grid needs nE >= 2, E_min > 0, E_fact > 0");
   if (g->nx < 2 || g->ny < 2 || g->nz < 2)
     return fail(h, HXG_ERR_INVALID, "grid needs at least 2 vertices per axis");
   if (!(g->x_max > g->x_min) || !(g->y_max > g->y_min) || !(g->z_max > g->z_min))
@@ -634,7 +747,7 @@ int upload_common(hxg_handle *h, int field, const hxg_grid_desc_t *g,
   for (int k = 0; k < (vec ? 3 : 1); ++k)
     if (!src[k]) return fail(h, HXG_ERR_INVALID, "grid component %d is NULL", k);
   Slot &S = h->slots[field];
-  const size_t n = (size_t)g->nx * g->ny * g->nz;
+  const size_t n = (size_t)g->nx * g->ny * g->nz * (field == HXG_FIELD_CRE ? g->nE : 1);
   if (S.present && S.n != n) {
     for (auto &p : S.d)
       if (p) cudaFree(p);
@@ -823,6 +936,8 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
   if (!h->have_models) return fail(h, HXG_ERR_STATE, "models not set");
   if (o->do_sync && h->models.cre == HXG_CRE_NONE)
     return fail(h, HXG_ERR_INVALID, "synchrotron output needs a CRE model");
+  if (o->do_sync && h->models.cre == HXG_CRE_GRID && !h->slots[HXG_FIELD_CRE].present)
+    return fail(h, HXG_ERR_STATE, "CRE grid model without an uploaded CRE grid");
   if ((o->do_dm && !d_dm) || (o->do_fd && !d_fd) ||
       (o->do_sync && (!d_is || !d_qs || !d_us)))
     return fail(h, HXG_ERR_INVALID, "an output requested by obs is NULL");
@@ -846,7 +961,7 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
     HXG_CK(cudaMemsetAsync(d_us, 0, b, h->stream));
   }
   const ExtModels *ext_dev = nullptr;
-  if ((st = upload_ext(h, h->models, &ext_dev)) != HXG_OK) return st;
+  if ((st = upload_ext(h, h->models, o->sync_freq, &ext_dev)) != HXG_OK) return st;
   for (uint32_t s = 0; s < o->total_shell; ++s) {
     ShellLaunch P;
     uint64_t step;
@@ -979,8 +1094,10 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
       return st;
   double *gs[5];
   for (int k = 0; k < 5; ++k) gs[k] = static_cast<double *>(h->g_shell[k].p);
+  if (h->models.cre == HXG_CRE_GRID)
+    return fail(h, HXG_ERR_UNSUPPORTED, "the adjoint does not cover the CRE-grid emissivity");
   const ExtModels *ext_dev = nullptr;
-  if ((st = upload_ext(h, h->models, &ext_dev)) != HXG_OK) return st;
+  if ((st = upload_ext(h, h->models, o->sync_freq, &ext_dev)) != HXG_OK) return st;
   for (int s = (int)o->total_shell - 1; s >= 0; --s) {
     ShellLaunch F;
     uint64_t step;
@@ -1256,6 +1373,16 @@ int hxg_los_geometry(uint64_t n, const double *theta, const double *phi,
   KAT_CK(cudaMemcpy(b_per, dper, n * 8, cudaMemcpyDeviceToHost));
   KAT_CK(cudaMemcpy(cos2ipa, dc, n * 8, cudaMemcpyDeviceToHost));
   KAT_CK(cudaMemcpy(sin2ipa, ds, n * 8, cudaMemcpyDeviceToHost));
+  return HXG_OK;
+}
+
+int hxg_synchrotron(int which, uint64_t n, const double *x, double *out) {
+  if ((which != 1 && which != 2) || (n > 0 && (!x || !out))) return HXG_ERR_INVALID;
+  const std::vector<double> &tab = synchro_tables();
+  const double *t = tab.data() + (which == 1 ? 0 : kSynchroN);
+  const double inv_du = (kSynchroN - 1) / (kSynchroU1 - kSynchroU0);
+  for (uint64_t i = 0; i < n; ++i)
+    out[i] = x[i] > 0. ? synchro_fn(t, kSynchroU0, inv_du, kSynchroN, x[i]) : 0.;
   return HXG_OK;
 }
 
@@ -1572,8 +1699,12 @@ int hxg_batch_create(hxg_handle *h, int n, const hxg_batch_entry_t *entries,
     for (size_t i = 0; i < b->e.size(); ++i) {
       if (!uses_ext(b->e[i].models)) continue;
       b->ext_any = true;
-      ext_models(b->e[i].models, b->fp32 ? 1.0 / cgs::kpc : 1.0,
-                 b->fp32 ? 1.0 / cgs::fp32_bunit : 1.0, ext[i]);
+      const double L = b->fp32 ? 1.0 / cgs::kpc : 1.0;
+      const double Bu = b->fp32 ? 1.0 / cgs::fp32_bunit : 1.0;
+      ext_models(b->e[i].models, L, Bu, ext[i]);
+      if (b->e[i].models.cre == HXG_CRE_GRID &&
+          (st = cre_grid_block(h, L, Bu, b->e[i].obs.sync_freq, ext[i].cre)) != HXG_OK)
+        return bail(st);
     }
     if (b->ext_any && (st = upload_vec(h, b->ext, ext)) != HXG_OK) return bail(st);
   }

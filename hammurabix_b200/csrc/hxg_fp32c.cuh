@@ -272,47 +272,59 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw,
         const float yv = -(etx * bx + ety * by + etz * bz);
         const float rr = fmaf(xv, xv, yv * yv);
         const float cc2 = fmaf(xv, xv, -yv * yv), ss2 = 2.f * xv * yv;
-        float prof;
-        if (M.cre == kCreAna) {
-          // exp((R0 - r)/r0) sech^2(z/z0)
-          //   = 4 exp((R0 - r)/r0 - 2|z|/z0) / (1 + exp(-2|z|/z0))^2
-          const float r2f = fmaf(xf, xf, yf * yf);
-          const float rf = r2f * rsqrtf(fmaxf(r2f, 1e-30f));
-          const float az2 = fabsf(zf) * cre_2iz0;
-          const float t = __expf(-az2);
-          const float den = 1.f + t;
-          prof = __fdividef(4.f * __expf((cre_R0 - rf) * cre_ir0 - az2), den * den);
-        } else {
-          prof = cre_profile<float>(M, xf, yf, zf, p3);
-        }
         float wt, wpc, wps;
-        if (pe2) {
-          wt = prof * rr;
-          wpc = prof * cc2;
-          wps = prof * ss2;
-        } else {
-          float wp;
-          if (P.em_const) {
-            const float bp = (pe == 1.f) ? sqrtf(rr) : powf(rr, 0.5f * pe);
-            wt = wp = prof * bp;
-          } else {
-            const float index = cre_index<float>(M, xf, yf, zf);
-            if (index != last_index) {
-              gt = tgammaf(-0.25f * index + 19.f / 12.f) * tgammaf(-0.25f * index - 1.f / 12.f);
-              gp = tgammaf(-0.25f * index + 7.f / 12.f) * tgammaf(-0.25f * index - 1.f / 12.f);
-              inv1mi = 1.f / (1.f - index);
-              last_index = index;
-            }
-            const float bper = sqrtf(rr);
-            const float Ae = exp2f(0.5f * (index + 1.f) * log2f(a_s / bper));
-            const float base = prof * bper * Ae;
-            wt = base * gt * inv1mi;
-            wp = base * gp;
-          }
-          // ipa of a zero B_perp is 0 (atan2(0, 0)): cos 2ipa = 1
+        if (kExt && M.cre == kCreGrid) {
+          // spectral integral over the CRE grid in FP64 (integrator.cc:288-330,
+          // 357-400); scaled by 2^128 into FP32 range, k_t = k_p undo it
+          double jt, jp;
+          cre_grid_j(P.ext->cre, px, py, pz, double(sqrtf(rr)), jt, jp);
+          wt = float(jt * 0x1p128);
+          const float wp = float(jp * 0x1p128);
           const float inv = rr > 0.f ? __frcp_rn(rr) : 0.f;
           wpc = rr > 0.f ? wp * cc2 * inv : wp;
           wps = wp * ss2 * inv;
+        } else {
+          float prof;
+          if (M.cre == kCreAna) {
+            // exp((R0 - r)/r0) sech^2(z/z0)
+            //   = 4 exp((R0 - r)/r0 - 2|z|/z0) / (1 + exp(-2|z|/z0))^2
+            const float r2f = fmaf(xf, xf, yf * yf);
+            const float rf = r2f * rsqrtf(fmaxf(r2f, 1e-30f));
+            const float az2 = fabsf(zf) * cre_2iz0;
+            const float t = __expf(-az2);
+            const float den = 1.f + t;
+            prof = __fdividef(4.f * __expf((cre_R0 - rf) * cre_ir0 - az2), den * den);
+          } else {
+            prof = cre_profile<float>(M, xf, yf, zf, p3);
+          }
+          if (pe2) {
+            wt = prof * rr;
+            wpc = prof * cc2;
+            wps = prof * ss2;
+          } else {
+            float wp;
+            if (P.em_const) {
+              const float bp = (pe == 1.f) ? sqrtf(rr) : powf(rr, 0.5f * pe);
+              wt = wp = prof * bp;
+            } else {
+              const float index = cre_index<float>(M, xf, yf, zf);
+              if (index != last_index) {
+                gt = tgammaf(-0.25f * index + 19.f / 12.f) * tgammaf(-0.25f * index - 1.f / 12.f);
+                gp = tgammaf(-0.25f * index + 7.f / 12.f) * tgammaf(-0.25f * index - 1.f / 12.f);
+                inv1mi = 1.f / (1.f - index);
+                last_index = index;
+              }
+              const float bper = sqrtf(rr);
+              const float Ae = exp2f(0.5f * (index + 1.f) * log2f(a_s / bper));
+              const float base = prof * bper * Ae;
+              wt = base * gt * inv1mi;
+              wp = base * gp;
+            }
+            // ipa of a zero B_perp is 0 (atan2(0, 0)): cos 2ipa = 1
+            const float inv = rr > 0.f ? __frcp_rn(rr) : 0.f;
+            wpc = rr > 0.f ? wp * cc2 * inv : wp;
+            wps = wp * ss2 * inv;
+          }
         }
         ki.add(wt);
         // Faraday phase: the turn count rev0 + rev_k * FD in FP64, its

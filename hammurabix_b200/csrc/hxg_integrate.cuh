@@ -247,31 +247,40 @@ __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
       if (P.do_dm) dm += te * P.delta;
       if (P.do_fd || P.do_sync) fd += te * bpar * P.fd_fore * P.delta;
       if (P.do_sync) {
-        double index = P.em_index;
-        if (!P.em_const) {
-          index = cre_index<double>(M, px, py, pz);
-          if (index != last_index) {
-            gt = tgamma(-0.25 * index + 19. / 12.) * tgamma(-0.25 * index - 1. / 12.);
-            gp = tgamma(-0.25 * index + 7. / 12.) * tgamma(-0.25 * index - 1. / 12.);
-            last_index = index;
+        double jtot, jpol;
+        if (kExt && M.cre == kCreGrid) {
+          // spectral integral over the CRE grid (integrator.cc:288-330, 357-400)
+          double jt, jp;
+          cre_grid_j(P.ext->cre, px, py, pz, bper, jt, jp);
+          jtot = jt * P.delta * P.i2bt;
+          jpol = jp * P.delta * P.i2bt;
+        } else {
+          double index = P.em_index;
+          if (!P.em_const) {
+            index = cre_index<double>(M, px, py, pz);
+            if (index != last_index) {
+              gt = tgamma(-0.25 * index + 19. / 12.) * tgamma(-0.25 * index - 1. / 12.);
+              gp = tgamma(-0.25 * index + 7. / 12.) * tgamma(-0.25 * index - 1. / 12.);
+              last_index = index;
+            }
           }
+          const double fn = P.em_n0u * cre_profile<double>(M, px, py, pz, p3);
+          const double absb = fabs(bper);
+          const double A = P.em_anum / (P.em_3qe * absb);
+          double Ae;
+          if (P.em_const && P.em_pow_kind == 1)
+            Ae = 1. / A;
+          else if (P.em_const && P.em_pow_kind == 2)
+            Ae = 1.;
+          else
+            Ae = pow(A, 0.5 * (index + 1));
+          const double den_t = P.em_const ? P.em_den_t
+                                          : 4. * cgs::pi * cgs::mec2 * (1. - index);
+          const double norm_t = fn * 1.73205081 * P.em_qe3 * absb / den_t;
+          const double norm_p = fn * 1.73205081 * P.em_qe3 * absb / P.em_den_p;
+          jtot = norm_t * (Ae * gt) * P.delta * P.i2bt;
+          jpol = norm_p * (Ae * gp) * P.delta * P.i2bt;
         }
-        const double fn = P.em_n0u * cre_profile<double>(M, px, py, pz, p3);
-        const double absb = fabs(bper);
-        const double A = P.em_anum / (P.em_3qe * absb);
-        double Ae;
-        if (P.em_const && P.em_pow_kind == 1)
-          Ae = 1. / A;
-        else if (P.em_const && P.em_pow_kind == 2)
-          Ae = 1.;
-        else
-          Ae = pow(A, 0.5 * (index + 1));
-        const double den_t = P.em_const ? P.em_den_t
-                                        : 4. * cgs::pi * cgs::mec2 * (1. - index);
-        const double norm_t = fn * 1.73205081 * P.em_qe3 * absb / den_t;
-        const double norm_p = fn * 1.73205081 * P.em_qe3 * absb / P.em_den_p;
-        const double jtot = norm_t * (Ae * gt) * P.delta * P.i2bt;
-        const double jpol = norm_p * (Ae * gp) * P.delta * P.i2bt;
         si += jtot;
         double c2, s2;
         ipa2<double>(-(epx * B.x + epy * B.y), -(etx * B.x + ety * B.y + etz * B.z),

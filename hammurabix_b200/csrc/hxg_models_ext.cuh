@@ -396,13 +396,99 @@ static __device__ __noinline__ double tereg_ymw16(const Ymw16Dev &Y, double x, d
          (w_lb) * (ne_comp[6]);
 }
 
-// The three models' parameter blocks of one launch, in device memory (the
-// kernels that read them are separate instantiations, so the common path
-// carries neither their code nor their parameters).
+// ---- CRE-grid synchrotron emissivity ---------------------------------
+// (integrator.cc:282-330 total, 351-400 polarised; CREfield::read_grid_num,
+// cre.cc:144-199).  The energy integral uses the midpoint rule over the
+// grid's energy bins with F(x) (total) and G(x) (polarised); both come from
+// tables of ln(F(x)/x^(1/3)), ln(G(x)/x^(1/3)) on u = ln x (smooth in u, so
+// the relative error stays uniform where F decays like e^-x), built on the
+// host from the integral definitions and read with 4-point Lagrange
+// interpolation.
+struct CreGridDev {
+  const double *flux;         // [((i*ny + j)*nz + k)*nE + e], (GeV m^2 s sr)^-1
+  int nx, ny, nz, nE;
+  double lo[3], hi[3];        // box (working length units)
+  const double *inv_ke2;      // [nE] 1 / KE_e^2, KE_e = E_min exp(e E_fact) (erg)
+  const double *beta;         // [nE] sqrt(1 - mec2 / KE_e)
+  const double *dke;          // [nE - 1] |KE_{e+1} - KE_e|
+  const double *tab_f, *tab_g;
+  double u0, inv_du;          // table abscissae u_k = u0 + k / inv_du
+  int ntab, _pad;
+  double xnum_t, xnum_p;      // numerators of x_fact (t, p) in the reference's order
+  double fore_num, fore_den;  // 1.73205081 qe^3 ; mec2 c GeV m^2 s
+  double bunit;               // G per working field unit
+};
+
+// F(x) or G(x) from its table: tab[k] = ln(fn(x_k) / x_k^(1/3)), x_k = e^(u0+k du)
+__host__ __device__ __forceinline__ double synchro_fn(const double *tab, double u0,
+                                                      double inv_du, int n, double x) {
+  const double t = (log(x) - u0) * inv_du;
+  if (!(t >= 1.)) return exp(tab[0]) * cbrt(x);  // below the table: x^(1/3) law
+  const int k = (int)t < n - 3 ? (int)t : n - 3;
+  const double f = t - k;
+  const double wm = -f * (f - 1.) * (f - 2.) * (1. / 6.);
+  const double w0 = (f + 1.) * (f - 1.) * (f - 2.) * 0.5;
+  const double w1 = -(f + 1.) * f * (f - 2.) * 0.5;
+  const double w2 = (f + 1.) * f * (f - 1.) * (1. / 6.);
+  return exp(wm * tab[k - 1] + w0 * tab[k] + w1 * tab[k + 1] + w2 * tab[k + 2]) * cbrt(x);
+}
+
+// J_tot and J_pol (erg s^-1 cm^-3 Hz^-1 sr^-1, before the step and the
+// brightness conversion) at position p for |B_perp| = bper (working units)
+static __device__ __noinline__ void cre_grid_j(const CreGridDev &C, double px, double py,
+                                        double pz, double bper, double &jt, double &jp) {
+  jt = jp = 0.;
+  const double p[3] = {px, py, pz};
+  const int n[3] = {C.nx, C.ny, C.nz};
+  int il[3];
+  double fr[3];
+  for (int a = 0; a < 3; ++a) {
+    const double tmp = (n[a] - 1) * (p[a] - C.lo[a]) / (C.hi[a] - C.lo[a]);
+    if (tmp <= 0 || tmp >= n[a] - 1) return;  // read_grid_num returns 0
+    il[a] = (int)floor(tmp);
+    fr[a] = tmp - il[a];
+  }
+  const double b = fabs(bper) * C.bunit;
+  const double xf_t = C.xnum_t / (3. * cgs::qe * b);
+  const double xf_p = C.xnum_p / (3. * cgs::qe * b);
+  const long long sz = (long long)C.nz * C.nE, sy = (long long)C.ny * sz;
+  const double *c000 = C.flux + il[0] * sy + il[1] * sz + (long long)il[2] * C.nE;
+  const double xd = fr[0], yd = fr[1], zd = fr[2];
+  // trilinear flux at energy e in read_grid_num's order: z, then y, then x
+  const auto flux_at = [&](int e) {
+    const double *q = c000 + e;
+    const double i1 = q[0] * (1. - zd) + q[C.nE] * zd;
+    const double i2 = q[sz] * (1 - zd) + q[sz + C.nE] * zd;
+    const double j1 = q[sy] * (1 - zd) + q[sy + C.nE] * zd;
+    const double j2 = q[sy + sz] * (1 - zd) + q[sy + sz + C.nE] * zd;
+    const double w1 = i1 * (1 - yd) + i2 * yd;
+    const double w2 = j1 * (1 - yd) + j2 * yd;
+    return w1 * (1 - xd) + w2 * xd;
+  };
+  double v_lo = flux_at(0) / C.beta[0];
+  double st = 0., sp = 0.;
+  for (int e = 0; e < C.nE - 1; ++e) {
+    const double v_hi = flux_at(e + 1) / C.beta[e + 1];
+    const double flux = 0.5 * (v_hi + v_lo);
+    v_lo = v_hi;
+    const double xt = 0.5 * (xf_t * C.inv_ke2[e + 1] + xf_t * C.inv_ke2[e]);
+    const double xp = 0.5 * (xf_p * C.inv_ke2[e + 1] + xf_p * C.inv_ke2[e]);
+    if (!(xt > 100)) st += synchro_fn(C.tab_f, C.u0, C.inv_du, C.ntab, xt) * flux * C.dke[e];
+    if (!(xp > 100)) sp += synchro_fn(C.tab_g, C.u0, C.inv_du, C.ntab, xp) * flux * C.dke[e];
+  }
+  const double fore = C.fore_num * b / C.fore_den;
+  jt = st * fore;
+  jp = sp * fore;
+}
+
+// The three models' parameter blocks and the CRE grid of one launch, in
+// device memory (the kernels that read them are separate instantiations, so
+// the common path carries neither their code nor their parameters).
 struct ExtModels {
   JaffeDev jaffe;
   Jf12Dev jf12;
   Ymw16Dev ymw16;
+  CreGridDev cre;
 };
 
 }  // namespace hxg

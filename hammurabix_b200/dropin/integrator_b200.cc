@@ -49,7 +49,7 @@ void check(int st, hxg_handle *h, const char *what) {
 // (Pipeline::assemble_obs calls write_grid once per <sync> entry).
 struct DeviceState {
   hxg_handle *h = nullptr;
-  const void *uploaded[4] = {nullptr, nullptr, nullptr, nullptr};
+  const void *uploaded[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   ~DeviceState() {
     if (h) hxg_destroy(h);
   }
@@ -95,7 +95,7 @@ hxg_models_t map_models(DeviceState &s, const Breg *breg, const Brnd *,
                         const TEreg *tereg, const TErnd *, const CREfield *cre,
                         const Grid_breg *gbreg, const Grid_brnd *gbrnd,
                         const Grid_tereg *gtereg, const Grid_ternd *gternd,
-                        const Param *par) {
+                        const Grid_cre *gcre, const Param *par) {
   hxg_models_t m{};
   // regular B
   if (par->grid_breg.read_permission) {
@@ -203,7 +203,18 @@ hxg_models_t map_models(DeviceState &s, const Breg *breg, const Brnd *,
   }
   // cosmic-ray electrons
   if (par->grid_cre.read_permission) {
-    throw std::runtime_error("hammurabiX-B200: CRE grids are not supported on the GPU");
+    // CRE_num: spectral integral over the CRE grid (integrator.cc:288-330)
+    m.cre = HXG_CRE_GRID;
+    if (s.uploaded[HXG_FIELD_CRE] != gcre->cre_flux.get()) {
+      hxg_grid_desc_t d = desc_of(par->grid_cre);
+      d.nE = static_cast<uint32_t>(par->grid_cre.nE);
+      d.E_min = par->grid_cre.E_min;
+      d.E_max = par->grid_cre.E_max;
+      d.E_fact = par->grid_cre.E_fact;
+      check(hxg_upload_grid(s.h, HXG_FIELD_CRE, &d, gcre->cre_flux.get(), nullptr, nullptr),
+            s.h, "hxg_upload_grid");
+      s.uploaded[HXG_FIELD_CRE] = gcre->cre_flux.get();
+    }
   } else if (dynamic_cast<const CRE_ana *>(cre)) {
     m.cre = HXG_CRE_ANA;
     m.cre_ana = {par->cre_ana.alpha, par->cre_ana.beta, par->cre_ana.theta,
@@ -259,11 +270,11 @@ void Integrator::write_grid(const Breg *breg, const Brnd *brnd,
                             const TEreg *tereg, const TErnd *ternd,
                             const CREfield *cre, const Grid_breg *gbreg,
                             const Grid_brnd *gbrnd, const Grid_tereg *gtereg,
-                            const Grid_ternd *gternd, const Grid_cre *,
+                            const Grid_ternd *gternd, const Grid_cre *gcre,
                             Grid_obs *gobs, const Param *par) const {
   DeviceState &s = state();
   const hxg_models_t m = map_models(s, breg, brnd, tereg, ternd, cre, gbreg, gbrnd,
-                                    gtereg, gternd, par);
+                                    gtereg, gternd, gcre, par);
   check(hxg_set_models(s.h, &m), s.h, "hxg_set_models");
   const hxg_obs_t o = map_obs(par);
   if (o.do_mask) {

@@ -222,6 +222,16 @@ def accumulate(nside_dst, dst, nside_src, src):
     return dst
 
 
+def synchrotron(which, x):
+    """F(x) (which=1) or G(x) (which=2) from the library's tables
+    (hxg_synchrotron)."""
+    lib = _lib.load()
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    out = np.zeros_like(x)
+    _lib.check(lib.hxg_synchrotron(int(which), len(x), _lib.dptr(x), _lib.dptr(out)))
+    return out
+
+
 def los_geometry(theta, phi, b):
     lib = _lib.load()
     theta = np.ascontiguousarray(theta, dtype=np.float64)

@@ -358,6 +358,11 @@ int hxg_write_grid_noalloc(const hxg_obs_t *obs, const hxg_models_t *models,
                            double *d_us, void *stream);
 
 /* ---- host helpers ------------------------------------------------------*/
+/* The synchrotron functions the CRE-grid emissivity integrates
+ * (gsl_sf_synchrotron_1 / _2 at integrator.cc:320, 396): which = 1:
+ * F(x) = x Int_x^inf K_{5/3}(t) dt, which = 2: G(x) = x K_{2/3}(x), from the
+ * same tables and interpolation the device uses; 0 for x <= 0.            */
+int hxg_synchrotron(int which, uint64_t n, const double *x, double *out);
 /* Integrator::assemble_shell_ref (integrator.cc:231-254): step count,
  * radial step and start distance of shell `shell`.                        */
 int hxg_shell_ref(const hxg_obs_t *obs, uint32_t shell, double *d_start,

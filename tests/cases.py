@@ -143,3 +143,28 @@ def case_dm_only():
     m = W.grid_models()
     m.ternd = abi.HXG_TERND_GRID
     return [o], m, g, None
+
+
+def case_cre_grid():
+    """Power-law CRE flux on a 9 x 9 x 5 box grid with 8 energies from 2 to
+    200 GeV: flux(E, pos) = 1e-2 (E / 10 GeV)^-3 exp(-r/8 kpc) sech^2(z/1 kpc)
+    (GeV m^2 s sr)^-1, with the analytic spiral B and exponential n_e."""
+    nx, ny, nz, nE = 9, 9, 5, 8
+    d = abi.GridDesc()
+    d.nx, d.ny, d.nz, d.nE = nx, ny, nz, nE
+    d.x_min, d.x_max = -20. * U.kpc, 20. * U.kpc
+    d.y_min, d.y_max = -20. * U.kpc, 20. * U.kpc
+    d.z_min, d.z_max = -4. * U.kpc, 4. * U.kpc
+    d.E_min = 2. * U.GeV
+    d.E_max = 200. * U.GeV
+    d.E_fact = np.log(d.E_max / d.E_min) / (nE - 1)
+    x = np.linspace(-20, 20, nx)[:, None, None, None]
+    y = np.linspace(-20, 20, ny)[None, :, None, None]
+    z = np.linspace(-4, 4, nz)[None, None, :, None]
+    E = (d.E_min * np.exp(np.arange(nE) * d.E_fact) / U.GeV)[None, None, None, :]
+    r = np.sqrt(x * x + y * y)
+    flux = 1e-2 * (E / 10.) ** -3 * np.exp(-r / 8.) / np.cosh(z) ** 2
+    m = W.spiral_models()
+    m.cre = abi.HXG_CRE_GRID
+    passes = [W.make_obs([8, 16], 20.0, 0.05, freq_ghz=f) for f in (1.4, 0.408)]
+    return passes, m, {abi.HXG_FIELD_CRE: (d, [np.ascontiguousarray(flux.reshape(-1))])}

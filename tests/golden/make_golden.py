@@ -16,6 +16,9 @@ that holds the hammurabiX source tree; the outputs are committed).
    reference's templates/params_template.xml (parsed by
    hammurabix_b200.param with Param's unit conversions); the hxg_models_t
    block of each case is stored beside its maps.
+5. ref_cre_grid.npz -- the same for the CRE-grid emissivity on the power-law
+   CRE grid of tests/cases.py:case_cre_grid (the reference built with the
+   oracle's F and G, oracle/shim/shim.cc).
 
 Usage: python tests/golden/make_golden.py [hammurabiX source dir]
 """
@@ -112,10 +115,18 @@ def reference_models_ext(src):
     np.savez_compressed(os.path.join(HERE, "ref_models_ext.npz"), **out)
 
 
+def reference_cre_grid():
+    ref = pyoracle.Reference()
+    out = {}
+    _run(ref, *cases.case_cre_grid(), None, "cre_grid", out)
+    np.savez_compressed(os.path.join(HERE, "ref_cre_grid.npz"), **out)
+
+
 if __name__ == "__main__":
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     reference_fixtures(src)
     reference_maps()
     reference_models_ext(src)
+    reference_cre_grid()
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))
