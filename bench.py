@@ -132,18 +132,14 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def setup_dist(args):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
+def setup_dist(args, gpu=True):
+    from hammurabix_b200 import replicas
+    ws, rank, local = replicas.env()
+    if ws > 1 and gpu:
         import torch
-        import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-    return ws, rank, local
+        return replicas.init("nccl", 600, torch.device("cuda", local))
+    return replicas.init("gloo", 600) if ws > 1 else (ws, rank, local)
 
 
 def make_passes(wl, nside_shells=None):
@@ -177,7 +173,9 @@ def cpu_baseline(wl, host_fields, steps=1):
 
 
 def run_reference_arm(args, wl):
-    ws, rank, _ = setup_dist(args)
+    # CPU only: no process group is needed; rank 0 alone runs and prints
+    from hammurabix_b200 import replicas
+    ws, rank, _ = replicas.env()
     if rank != 0:
         return
     import numpy as np
@@ -348,6 +346,7 @@ def main():
     from hammurabix_b200 import abi, workloads as W
     from hammurabix_b200.integrator import Integrator
 
+    from hammurabix_b200 import replicas
     ws, rank, local = setup_dist(args)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -386,8 +385,7 @@ def main():
 
     def barrier():
         torch.cuda.synchronize(dev)
-        if ws > 1:
-            torch.distributed.barrier()
+        replicas.barrier(ws)
 
     def timed(ig, outs, k):
         ev0 = torch.cuda.Event(enable_timing=True)
@@ -401,11 +399,7 @@ def main():
         return ev0.elapsed_time(ev1) / 1e3
 
     def max_over_ranks(x):
-        if ws == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return t.item()
+        return replicas.max_over_ranks(x, ws, dev)
 
     # ---- FP32-compensated form: the product path ------------------------
     ig32 = make_integ("fp32c")
@@ -419,7 +413,7 @@ def main():
     launches = ig32.launch_count() - lc0
     kms, klaunch, ksamples = ig32.get_timing()
     ig32.set_timing(False)
-    value = ws * samples_step * args.steps / t32
+    value = replicas.throughput(samples_step * args.steps, ws, t32)
     ms_step = t32 / args.steps * 1e3
     log(f"[rank {rank}] fp32c: {ms_step:.1f} ms/step, {value:.4g} samples/s")
 
@@ -561,8 +555,7 @@ def main():
         }
         print(json.dumps(line), flush=True)
     ig32.close()
-    if ws > 1:
-        torch.distributed.destroy_process_group()
+    replicas.finish(ws)
 
 
 if __name__ == "__main__":
