@@ -46,6 +46,7 @@ SIGNATURES = {
     "hxg_accumulate": (C.c_int, [C.c_uint32, _dp, C.c_uint32, _dp]),
     "hxg_los_geometry": (C.c_int, [C.c_uint64, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     "hxg_read_grid": (C.c_int, [_h, C.c_int, C.c_uint64, _dp, _dp]),
+    "hxg_upload_grid_file": (C.c_int, [_h, C.c_int, C.POINTER(abi.GridDesc), C.c_char_p]),
     "hxg_synchrotron": (C.c_int, [C.c_int, C.c_uint64, _dp, _dp]),
     "hxg_batch_create": (C.c_int, [_h, C.c_int, C.POINTER(abi.BatchEntry), C.c_int,
                                    C.POINTER(_vp)]),

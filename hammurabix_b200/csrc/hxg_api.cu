@@ -730,10 +730,12 @@ int validate_obs(hxg_handle *h, const hxg_obs_t *o) {
   return HXG_OK;
 }
 
-int upload_common(hxg_handle *h, int field, const hxg_grid_desc_t *g,
-                  const double *c0, const double *c1, const double *c2,
-                  cudaMemcpyKind kind) {
-  if (!h) return HXG_ERR_INVALID;
+// Validate a grid descriptor for slot `field` and (re)allocate the slot's
+// device arrays: 3 components for the B slots, 1 otherwise; the CRE slot
+// holds nx*ny*nz*nE values.  The slot is marked present by the caller once
+// its data are in place.
+int slot_prepare(hxg_handle *h, int field, const hxg_grid_desc_t *g, size_t *n_out,
+                 int *ncomp_out) {
   if (field < 0 || field > HXG_FIELD_CRE || !g)
     return fail(h, HXG_ERR_INVALID, "bad field slot %d", field);
   if (field == HXG_FIELD_CRE && (g->nE < 2 || !(g->E_fact > 0.) || !(g->E_min > 0.)))
@@ -742,10 +744,7 @@ int upload_common(hxg_handle *h, int field, const hxg_grid_desc_t *g,
     return fail(h, HXG_ERR_INVALID, "grid needs at least 2 vertices per axis");
   if (!(g->x_max > g->x_min) || !(g->y_max > g->y_min) || !(g->z_max > g->z_min))
     return fail(h, HXG_ERR_INVALID, "grid box has non-positive extent");
-  const bool vec = field == HXG_FIELD_BREG || field == HXG_FIELD_BRND;
-  const double *src[3] = {c0, c1, c2};
-  for (int k = 0; k < (vec ? 3 : 1); ++k)
-    if (!src[k]) return fail(h, HXG_ERR_INVALID, "grid component %d is NULL", k);
+  const int ncomp = (field == HXG_FIELD_BREG || field == HXG_FIELD_BRND) ? 3 : 1;
   Slot &S = h->slots[field];
   const size_t n = (size_t)g->nx * g->ny * g->nz * (field == HXG_FIELD_CRE ? g->nE : 1);
   if (S.present && S.n != n) {
@@ -753,16 +752,36 @@ int upload_common(hxg_handle *h, int field, const hxg_grid_desc_t *g,
       if (p) cudaFree(p);
     S.d[0] = S.d[1] = S.d[2] = nullptr;
   }
-  for (int k = 0; k < (vec ? 3 : 1); ++k) {
+  S.present = false;
+  for (int k = 0; k < ncomp; ++k) {
     if (!S.d[k]) {
       cudaError_t e = cudaMalloc(&S.d[k], n * sizeof(double));
       if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc(grid)");
     }
-    HXG_CK(cudaMemcpyAsync(S.d[k], src[k], n * sizeof(double), kind, h->stream));
   }
-  S.present = true;
   S.n = n;
   S.desc = *g;
+  *n_out = n;
+  *ncomp_out = ncomp;
+  return HXG_OK;
+}
+
+int upload_common(hxg_handle *h, int field, const hxg_grid_desc_t *g,
+                  const double *c0, const double *c1, const double *c2,
+                  cudaMemcpyKind kind) {
+  if (!h) return HXG_ERR_INVALID;
+  const bool vec = field == HXG_FIELD_BREG || field == HXG_FIELD_BRND;
+  const double *src[3] = {c0, c1, c2};
+  for (int k = 0; k < (vec ? 3 : 1); ++k)
+    if (!src[k]) return fail(h, HXG_ERR_INVALID, "grid component %d is NULL", k);
+  size_t n;
+  int ncomp;
+  int st = slot_prepare(h, field, g, &n, &ncomp);
+  if (st != HXG_OK) return st;
+  Slot &S = h->slots[field];
+  for (int k = 0; k < ncomp; ++k)
+    HXG_CK(cudaMemcpyAsync(S.d[k], src[k], n * sizeof(double), kind, h->stream));
+  S.present = true;
   h->groups_dirty = true;
   return HXG_OK;
 }
@@ -909,6 +928,75 @@ int hxg_upload_grid_device(hxg_handle *h, int field, const hxg_grid_desc_t *g,
   if (!h) return HXG_ERR_INVALID;
   cudaSetDevice(h->device);
   return upload_common(h, field, g, d_c0, d_c1, d_c2, cudaMemcpyDeviceToDevice);
+}
+
+int hxg_upload_grid_file(hxg_handle *h, int field, const hxg_grid_desc_t *g,
+                         const char *path) {
+  if (!h) return HXG_ERR_INVALID;
+  if (!path) return fail(h, HXG_ERR_INVALID, "path is NULL");
+  cudaSetDevice(h->device);
+  std::FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(h, HXG_ERR_INVALID, "cannot open %s", path);
+  struct Closer {
+    std::FILE *f;
+    ~Closer() { std::fclose(f); }
+  } closer{f};
+  size_t n;
+  int ncomp;
+  int st = slot_prepare(h, field, g, &n, &ncomp);
+  if (st != HXG_OK) return st;
+  const size_t total = n * (size_t)ncomp;  // doubles in the file
+  if (std::fseek(f, 0, SEEK_END) != 0) return fail(h, HXG_ERR_INVALID, "cannot seek %s", path);
+  const long bytes = std::ftell(f);
+  if (bytes < 0 || (size_t)bytes != total * sizeof(double))
+    return fail(h, HXG_ERR_INVALID, "%s holds %ld bytes, the grid needs %zu", path, bytes,
+                total * sizeof(double));
+  std::rewind(f);
+  // double-buffered chunks of 3 * 2^20 doubles (24 MiB, whole voxels for
+  // 3 components): read chunk k while chunk k-1 is copied and split
+  const size_t chunk = 3ull << 20;
+  struct Bufs {
+    void *pin[2] = {nullptr, nullptr};
+    double *stage[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    ~Bufs() {
+      for (int k = 0; k < 2; ++k) {
+        if (ev[k]) cudaEventSynchronize(ev[k]), cudaEventDestroy(ev[k]);
+        if (pin[k]) cudaFreeHost(pin[k]);
+        if (stage[k]) cudaFree(stage[k]);
+      }
+    }
+  } B;
+  for (int k = 0; k < 2; ++k) {
+    HXG_CK(cudaHostAlloc(&B.pin[k], chunk * sizeof(double), cudaHostAllocDefault));
+    if (ncomp == 3) HXG_CK(cudaMalloc(&B.stage[k], chunk * sizeof(double)));
+    HXG_CK(cudaEventCreateWithFlags(&B.ev[k], cudaEventDisableTiming));
+    HXG_CK(cudaEventRecord(B.ev[k], h->stream));
+  }
+  Slot &S = h->slots[field];
+  int k = 0;
+  for (size_t off = 0; off < total; off += chunk, k ^= 1) {
+    const size_t cnt = std::min(chunk, total - off);
+    HXG_CK(cudaEventSynchronize(B.ev[k]));  // pin[k] free again
+    if (std::fread(B.pin[k], sizeof(double), cnt, f) != cnt)
+      return fail(h, HXG_ERR_INVALID, "short read from %s", path);
+    if (ncomp == 1) {
+      HXG_CK(cudaMemcpyAsync(S.d[0] + off, B.pin[k], cnt * sizeof(double),
+                             cudaMemcpyHostToDevice, h->stream));
+    } else {
+      HXG_CK(cudaMemcpyAsync(B.stage[k], B.pin[k], cnt * sizeof(double),
+                             cudaMemcpyHostToDevice, h->stream));
+      const size_t v0 = off / 3;
+      HXG_CK(launch_deinterleave3(h->stream, cnt / 3, B.stage[k], S.d[0] + v0, S.d[1] + v0,
+                                  S.d[2] + v0));
+      ++h->launch_count;
+    }
+    HXG_CK(cudaEventRecord(B.ev[k], h->stream));
+  }
+  HXG_CK(cudaStreamSynchronize(h->stream));
+  S.present = true;
+  h->groups_dirty = true;
+  return HXG_OK;
 }
 
 int hxg_set_mask(hxg_handle *h, uint32_t nside, const double *mask) {

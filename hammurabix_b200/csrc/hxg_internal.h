@@ -50,6 +50,8 @@ cudaError_t launch_batch_merge(cudaStream_t s, const MergeJob *jobs,
 cudaError_t launch_batch_zero(cudaStream_t s, const ZeroJob *jobs,
                               const unsigned long long *block0, int njobs,
                               unsigned long long nblocks);
+cudaError_t launch_deinterleave3(cudaStream_t s, uint64_t n, const double *src, double *x,
+                                 double *y, double *z);
 cudaError_t launch_unpack_grad(cudaStream_t s, uint64_t n, const double *rec,
                                double *gbx, double *gby, double *gbz,
                                double *gne);

@@ -332,6 +332,24 @@ cudaError_t batch_level_occupancy(bool fp32, int ngroups, bool ext, int *blocks_
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, 256, 0);
 }
 
+// Split interleaved (x, y, z) voxel triples into three SoA arrays
+// (the on-disk layout of Grid_breg / Grid_brnd, grid_breg.cc:48-66).
+__global__ void deinterleave3_kernel(uint64_t n, const double *src, double *x, double *y,
+                                     double *z) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = src[3 * i];
+  y[i] = src[3 * i + 1];
+  z[i] = src[3 * i + 2];
+}
+
+cudaError_t launch_deinterleave3(cudaStream_t s, uint64_t n, const double *src, double *x,
+                                 double *y, double *z) {
+  if (n == 0) return cudaSuccess;
+  deinterleave3_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, src, x, y, z);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_batch_merge(cudaStream_t s, const MergeJob *jobs,
                                const unsigned long long *block0, int njobs,
                                unsigned long long nblocks) {

@@ -10,6 +10,7 @@ Device-resident inputs and outputs (torch CUDA tensors) go through
 ``upload_grid_device`` and ``write_grid_device``.
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -65,6 +66,12 @@ class Integrator:
         ptrs = [C.c_void_p(t.data_ptr()) for t in comps] + [None] * (3 - len(comps))
         _lib.check(self._lib.hxg_upload_grid_device(self._h, int(field), C.byref(desc),
                                                     *ptrs), self._h)
+
+    def upload_grid_file(self, field, desc, path):
+        """Load a grid from the reference's binary grid file
+        (hxg_upload_grid_file: chunked pinned reads, device-side split)."""
+        _lib.check(self._lib.hxg_upload_grid_file(self._h, field, C.byref(desc),
+                                                  os.fsencode(path)), self._h)
 
     def set_mask(self, nside, mask):
         m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)

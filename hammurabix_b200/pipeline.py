@@ -23,17 +23,6 @@ from .integrator import Integrator
 from .param import Param, ParamError
 
 
-def read_grid_file(path, desc, ncomp):
-    """Grid_*::import_grid: raw FP64, the ncomp components interleaved per
-    voxel; returns ncomp SoA arrays."""
-    n = int(desc.nx) * int(desc.ny) * int(desc.nz)
-    a = np.fromfile(path, dtype="<f8")
-    if a.size != n * ncomp:
-        raise ParamError(f"{path}: {a.size} values, expected {n * ncomp}")
-    a = a.reshape(n, ncomp)
-    return [np.ascontiguousarray(a[:, k]) for k in range(ncomp)]
-
-
 def _sync_freq_string(par, idx):
     """The frequency string of a <sync> entry as written in the XML (the key
     hampyx uses, hampyx.py:284-290)."""
@@ -65,8 +54,7 @@ class Pipeline:
             if not active:
                 continue
             desc, fname = par.grids[slot]
-            ncomp = 3 if slot in (abi.HXG_FIELD_BREG, abi.HXG_FIELD_BRND) else 1
-            self.integ.upload_grid(slot, desc, read_grid_file(fname, desc, ncomp))
+            self.integ.upload_grid_file(slot, desc, fname)
         if par.do_mask:
             mask = np.fromfile(par.mask_name, dtype="<f8")
             if mask.size != abi.npix(par.nside_mask):

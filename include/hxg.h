@@ -222,6 +222,16 @@ int hxg_set_models(hxg_handle *h, const hxg_models_t *m);
 int hxg_upload_grid(hxg_handle *h, int field, const hxg_grid_desc_t *g,
                     const double *c0, const double *c1, const double *c2);
 /* Same, from device-resident FP64 SoA arrays (no host copy).              */
+/* Load a grid straight from the reference's binary grid file
+ * (Grid_*::import_grid, source/grid/grid_breg.cc:48-66 and its tereg /
+ * brnd / ternd / cre twins): raw native-endian FP64, the B slots with
+ * (bx, by, bz) interleaved per voxel, x-major with z fastest; the CRE slot
+ * nx*ny*nz*nE values with the energy fastest.  The file is read in large
+ * chunks into pinned host buffers, copied while the next chunk is read, and
+ * split into components on the device.  A file whose size does not match
+ * the descriptor is rejected (HXG_ERR_INVALID).  Synchronous.              */
+int hxg_upload_grid_file(hxg_handle *h, int field, const hxg_grid_desc_t *g,
+                         const char *path);
 int hxg_upload_grid_device(hxg_handle *h, int field, const hxg_grid_desc_t *g,
                            const double *d_c0, const double *d_c1,
                            const double *d_c2);
