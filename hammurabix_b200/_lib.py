@@ -48,6 +48,12 @@ SIGNATURES = {
     "hxg_read_grid": (C.c_int, [_h, C.c_int, C.c_uint64, _dp, _dp]),
     "hxg_upload_grid_file": (C.c_int, [_h, C.c_int, C.POINTER(abi.GridDesc), C.c_char_p]),
     "hxg_synchrotron": (C.c_int, [C.c_int, C.c_uint64, _dp, _dp]),
+    "hxg_download_grid": (C.c_int, [_h, C.c_int, _dp, _dp, _dp]),
+    "hxg_export_grid_file": (C.c_int, [_h, C.c_int, C.c_char_p]),
+    "hxg_generate_brnd_es": (C.c_int, [_h, C.POINTER(abi.GridDesc), C.POINTER(abi.BrndEs),
+                                       _dp, C.c_uint64]),
+    "hxg_generate_ternd_dft": (C.c_int, [_h, C.POINTER(abi.GridDesc), C.POINTER(abi.TerndDft),
+                                         _dp, C.c_uint64]),
     "hxg_batch_create": (C.c_int, [_h, C.c_int, C.POINTER(abi.BatchEntry), C.c_int,
                                    C.POINTER(_vp)]),
     "hxg_batch_run": (C.c_int, [_vp]),

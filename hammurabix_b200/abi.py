@@ -110,6 +110,16 @@ class TeregYmw16(C.Structure):
                            "t7_detthetali", "t7_thetali"]))
 
 
+class BrndEs(C.Structure):
+    """hxg_brnd_es_t (Param::brnd_es)."""
+    _fields_ = _fields(["rms", "k0", "k1", "a0", "a1", "rho", "r0", "z0"])
+
+
+class TerndDft(C.Structure):
+    """hxg_ternd_dft_t (Param::ternd_dft)."""
+    _fields_ = _fields(["rms", "k0", "a0", "r0", "z0"])
+
+
 class CreAna(C.Structure):
     _fields_ = _fields(["alpha", "beta", "theta", "r0", "z0", "E0", "j0"])
 

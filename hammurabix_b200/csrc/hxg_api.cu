@@ -11,6 +11,9 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <chrono>
+#include <functional>
+#include <thread>
 #include <map>
 #include <mutex>
 #include <string>
@@ -994,6 +997,203 @@ int hxg_upload_grid_file(hxg_handle *h, int field, const hxg_grid_desc_t *g,
     HXG_CK(cudaEventRecord(B.ev[k], h->stream));
   }
   HXG_CK(cudaStreamSynchronize(h->stream));
+  S.present = true;
+  h->groups_dirty = true;
+  return HXG_OK;
+}
+
+int hxg_download_grid(hxg_handle *h, int field, double *c0, double *c1, double *c2) {
+  if (!h) return HXG_ERR_INVALID;
+  if (field < 0 || field > HXG_FIELD_CRE) return fail(h, HXG_ERR_INVALID, "bad field slot %d", field);
+  cudaSetDevice(h->device);
+  const Slot &S = h->slots[field];
+  if (!S.present) return fail(h, HXG_ERR_STATE, "grid slot %d is empty", field);
+  const int ncomp = (field == HXG_FIELD_BREG || field == HXG_FIELD_BRND) ? 3 : 1;
+  double *dst[3] = {c0, c1, c2};
+  for (int k = 0; k < ncomp; ++k)
+    if (!dst[k]) return fail(h, HXG_ERR_INVALID, "grid component %d is NULL", k);
+  for (int k = 0; k < ncomp; ++k)
+    HXG_CK(cudaMemcpyAsync(dst[k], S.d[k], S.n * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->stream));
+  HXG_CK(cudaStreamSynchronize(h->stream));
+  return HXG_OK;
+}
+
+int hxg_export_grid_file(hxg_handle *h, int field, const char *path) {
+  if (!h) return HXG_ERR_INVALID;
+  if (!path) return fail(h, HXG_ERR_INVALID, "path is NULL");
+  if (field < 0 || field > HXG_FIELD_CRE) return fail(h, HXG_ERR_INVALID, "bad field slot %d", field);
+  cudaSetDevice(h->device);
+  const Slot &S = h->slots[field];
+  if (!S.present) return fail(h, HXG_ERR_STATE, "grid slot %d is empty", field);
+  const int ncomp = (field == HXG_FIELD_BREG || field == HXG_FIELD_BRND) ? 3 : 1;
+  std::FILE *f = std::fopen(path, "wb");
+  if (!f) return fail(h, HXG_ERR_INVALID, "cannot create %s", path);
+  struct Closer {
+    std::FILE *f;
+    ~Closer() {
+      if (f) std::fclose(f);
+    }
+  } closer{f};
+  const size_t total = S.n * (size_t)ncomp;
+  // double-buffered chunks of 3 * 2^20 doubles: chunk k is interleaved and
+  // copied to pinned memory while chunk k-1 is written
+  const size_t chunk = 3ull << 20;
+  struct Bufs {
+    void *pin[2] = {nullptr, nullptr};
+    double *stage[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    ~Bufs() {
+      for (int k = 0; k < 2; ++k) {
+        if (ev[k]) cudaEventSynchronize(ev[k]), cudaEventDestroy(ev[k]);
+        if (pin[k]) cudaFreeHost(pin[k]);
+        if (stage[k]) cudaFree(stage[k]);
+      }
+    }
+  } B;
+  for (int k = 0; k < 2; ++k) {
+    HXG_CK(cudaHostAlloc(&B.pin[k], chunk * sizeof(double), cudaHostAllocDefault));
+    if (ncomp == 3) HXG_CK(cudaMalloc(&B.stage[k], chunk * sizeof(double)));
+    HXG_CK(cudaEventCreateWithFlags(&B.ev[k], cudaEventDisableTiming));
+  }
+  size_t cnt[2] = {0, 0};
+  auto flush = [&](int k) -> int {
+    HXG_CK(cudaEventSynchronize(B.ev[k]));
+    if (std::fwrite(B.pin[k], sizeof(double), cnt[k], f) != cnt[k])
+      return fail(h, HXG_ERR_INVALID, "short write to %s", path);
+    cnt[k] = 0;
+    return HXG_OK;
+  };
+  int k = 0;
+  for (size_t off = 0; off < total; off += chunk, k ^= 1) {
+    if (cnt[k]) {
+      const int st = flush(k);
+      if (st != HXG_OK) return st;
+    }
+    const size_t c = std::min(chunk, total - off);
+    if (ncomp == 1) {
+      HXG_CK(cudaMemcpyAsync(B.pin[k], S.d[0] + off, c * sizeof(double),
+                             cudaMemcpyDeviceToHost, h->stream));
+    } else {
+      const size_t v0 = off / 3;
+      HXG_CK(launch_interleave3(h->stream, c / 3, S.d[0] + v0, S.d[1] + v0, S.d[2] + v0,
+                                B.stage[k]));
+      ++h->launch_count;
+      HXG_CK(cudaMemcpyAsync(B.pin[k], B.stage[k], c * sizeof(double), cudaMemcpyDeviceToHost,
+                             h->stream));
+    }
+    HXG_CK(cudaEventRecord(B.ev[k], h->stream));
+    cnt[k] = c;
+  }
+  for (int j = 0; j < 2; ++j, k ^= 1)
+    if (cnt[k]) {
+      const int st = flush(k);
+      if (st != HXG_OK) return st;
+    }
+  if (std::fclose(f) != 0) {
+    closer.f = nullptr;
+    return fail(h, HXG_ERR_INVALID, "cannot close %s", path);
+  }
+  closer.f = nullptr;
+  return HXG_OK;
+}
+
+// ---- random-field generators ---------------------------------------------
+namespace {
+
+// toolkit::random_seed (include/toolkit.h:122-136): a given seed, or one
+// from the clock and the calling thread for 0.
+uint64_t rfg_seed(uint64_t seed) {
+  if (seed) return seed;
+  const auto now = std::chrono::system_clock::now();
+  const uint64_t t = (uint64_t)std::chrono::system_clock::to_time_t(now);
+  return t + (uint64_t)std::hash<std::thread::id>{}(std::this_thread::get_id());
+}
+
+bool finite_pos(double v) { return std::isfinite(v) && v > 0.; }
+
+int rfg_result(hxg_handle *h, int st, const char *what) {
+  if (st == HXG_OK) return st;
+  if (st == HXG_ERR_INVALID) return fail(h, st, "%s: the spectrum has no power on this grid", what);
+  if (st == HXG_ERR_OOM) return fail(h, st, "%s: out of device memory", what);
+  return fail(h, st, "%s: a CUDA or cuFFT call failed", what);
+}
+
+}  // namespace
+
+int hxg_generate_ternd_dft(hxg_handle *h, const hxg_grid_desc_t *g,
+                           const hxg_ternd_dft_t *p, const double observer[3],
+                           uint64_t seed) {
+  if (!h) return HXG_ERR_INVALID;
+  if (!g || !p || !observer) return fail(h, HXG_ERR_INVALID, "NULL argument");
+  if (!(std::isfinite(p->rms) && p->rms >= 0.) || !finite_pos(p->k0) ||
+      !std::isfinite(p->a0) || !finite_pos(p->r0) || !finite_pos(p->z0))
+    return fail(h, HXG_ERR_INVALID, "ternd_dft needs rms >= 0 and k0, r0, z0 > 0");
+  cudaSetDevice(h->device);
+  size_t n;
+  int ncomp;
+  int st = slot_prepare(h, HXG_FIELD_TERND, g, &n, &ncomp);
+  if (st != HXG_OK) return st;
+  Slot &S = h->slots[HXG_FIELD_TERND];
+  st = generate_ternd_dft(h->stream, *g, *p, observer, rfg_seed(seed), S.d[0]);
+  h->launch_count += 4;  // fill, two reduction passes, rescale
+  if (st != HXG_OK) return rfg_result(h, st, "ternd_dft");
+  S.present = true;
+  h->groups_dirty = true;
+  return HXG_OK;
+}
+
+int hxg_generate_brnd_es(hxg_handle *h, const hxg_grid_desc_t *g, const hxg_brnd_es_t *p,
+                         const double observer[3], uint64_t seed) {
+  if (!h) return HXG_ERR_INVALID;
+  if (!g || !p || !observer) return fail(h, HXG_ERR_INVALID, "NULL argument");
+  if (!(std::isfinite(p->rms) && p->rms >= 0.) || !finite_pos(p->k0) || !finite_pos(p->k1) ||
+      !std::isfinite(p->a0) || !std::isfinite(p->a1) || !finite_pos(p->rho) ||
+      !finite_pos(p->r0) || !finite_pos(p->z0))
+    return fail(h, HXG_ERR_INVALID, "brnd_es needs rms >= 0 and k0, k1, rho, r0, z0 > 0");
+  if (!h->have_models)
+    return fail(h, HXG_ERR_STATE, "models not set: the anisotropy follows the regular field");
+  cudaSetDevice(h->device);
+  const hxg_models_t &m = h->models;
+  RfgBregGrid bg{};
+  if (m.breg == HXG_BREG_GRID) {
+    const Slot &B = h->slots[HXG_FIELD_BREG];
+    if (!B.present) return fail(h, HXG_ERR_STATE, "BREG grid not uploaded");
+    bg.bx = B.d[0];
+    bg.by = B.d[1];
+    bg.bz = B.d[2];
+    bg.nx = (int)B.desc.nx;
+    bg.ny = (int)B.desc.ny;
+    bg.nz = (int)B.desc.nz;
+    bg.x_min = B.desc.x_min;
+    bg.x_max = B.desc.x_max;
+    bg.y_min = B.desc.y_min;
+    bg.y_max = B.desc.y_max;
+    bg.z_min = B.desc.z_min;
+    bg.z_max = B.desc.z_max;
+  }
+  const DevModels M = dev_models(m, observer, 1.0, 1.0);
+  // Jaffe / JF12 blocks in CGS for the anisotropy direction
+  struct ExtBuf {
+    ExtModels *p = nullptr;
+    ~ExtBuf() {
+      if (p) cudaFree(p);
+    }
+  } xb;
+  if (m.breg == HXG_BREG_JAFFE || m.breg == HXG_BREG_JF12) {
+    ExtModels x;
+    ext_models(m, 1.0, 1.0, x);
+    HXG_CK(cudaMalloc(&xb.p, sizeof(ExtModels)));
+    HXG_CK(cudaMemcpy(xb.p, &x, sizeof(x), cudaMemcpyHostToDevice));
+  }
+  size_t n;
+  int ncomp;
+  int st = slot_prepare(h, HXG_FIELD_BRND, g, &n, &ncomp);
+  if (st != HXG_OK) return st;
+  Slot &S = h->slots[HXG_FIELD_BRND];
+  st = generate_brnd_es(h->stream, *g, *p, M, xb.p, bg, rfg_seed(seed), S.d[0], S.d[1], S.d[2]);
+  h->launch_count += 7;  // fill, two reductions, rescale, project, repack, final
+  if (st != HXG_OK) return rfg_result(h, st, "brnd_es");
   S.present = true;
   h->groups_dirty = true;
   return HXG_OK;

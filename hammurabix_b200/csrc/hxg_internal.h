@@ -6,6 +6,8 @@
 
 #include <cstdint>
 
+#include "../../include/hxg.h"
+
 namespace hxg {
 
 struct ShellLaunch;
@@ -14,6 +16,16 @@ struct AdjointLaunch;
 struct BatchLevel;
 struct MergeJob;
 struct ZeroJob;
+struct DevModels;
+struct ExtModels;
+
+// The BREG slot as the Brnd_es anisotropy reads it (Breg::read_grid,
+// source/field/b/breg.cc:28-97): FP64 SoA vertex arrays in CGS.
+struct RfgBregGrid {
+  const double *bx, *by, *bz;  // null: the regular field is analytic
+  int nx, ny, nz;
+  double x_min, x_max, y_min, y_max, z_min, z_max;
+};
 
 cudaError_t launch_accumulate(cudaStream_t s, int nside_dst, int nside_src,
                               int nmaps, double *const *dst,
@@ -52,8 +64,17 @@ cudaError_t launch_batch_zero(cudaStream_t s, const ZeroJob *jobs,
                               unsigned long long nblocks);
 cudaError_t launch_deinterleave3(cudaStream_t s, uint64_t n, const double *src, double *x,
                                  double *y, double *z);
+cudaError_t launch_interleave3(cudaStream_t s, uint64_t n, const double *x, const double *y,
+                               const double *z, double *dst);
 cudaError_t launch_unpack_grad(cudaStream_t s, uint64_t n, const double *rec,
                                double *gbx, double *gby, double *gbz,
                                double *gne);
+
+// Random-field generators (hxg_rfg.cu); synchronous on s, HXG_* status.
+int generate_ternd_dft(cudaStream_t s, const hxg_grid_desc_t &g, const hxg_ternd_dft_t &p,
+                       const double obs[3], uint64_t seed, double *te);
+int generate_brnd_es(cudaStream_t s, const hxg_grid_desc_t &g, const hxg_brnd_es_t &p,
+                     const DevModels &M, const ExtModels *ext, const RfgBregGrid &breg,
+                     uint64_t seed, double *bx, double *by, double *bz);
 
 }  // namespace hxg

@@ -350,6 +350,24 @@ cudaError_t launch_deinterleave3(cudaStream_t s, uint64_t n, const double *src, 
   return cudaGetLastError();
 }
 
+// The inverse: three SoA arrays into (x, y, z) triples (Grid_brnd::export_grid,
+// grid_brnd.cc:57-73).
+__global__ void interleave3_kernel(uint64_t n, const double *x, const double *y,
+                                   const double *z, double *dst) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  dst[3 * i] = x[i];
+  dst[3 * i + 1] = y[i];
+  dst[3 * i + 2] = z[i];
+}
+
+cudaError_t launch_interleave3(cudaStream_t s, uint64_t n, const double *x, const double *y,
+                               const double *z, double *dst) {
+  if (n == 0) return cudaSuccess;
+  interleave3_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, x, y, z, dst);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_batch_merge(cudaStream_t s, const MergeJob *jobs,
                                const unsigned long long *block0, int njobs,
                                unsigned long long nblocks) {

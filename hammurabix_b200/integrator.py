@@ -73,6 +73,39 @@ class Integrator:
         _lib.check(self._lib.hxg_upload_grid_file(self._h, field, C.byref(desc),
                                                   os.fsencode(path)), self._h)
 
+    def download_grid(self, field, desc):
+        """A slot's FP64 SoA arrays as numpy arrays (hxg_download_grid),
+        shaped (nx, ny, nz) (flat for the CRE slot); desc is the slot's
+        geometry."""
+        vec = field in (abi.HXG_FIELD_BREG, abi.HXG_FIELD_BRND)
+        n = desc.nx * desc.ny * desc.nz * (desc.nE if field == abi.HXG_FIELD_CRE else 1)
+        out = [np.zeros(n) for _ in range(3 if vec else 1)]
+        ptrs = [_lib.dptr(a) for a in out] + [None] * (3 - len(out))
+        _lib.check(self._lib.hxg_download_grid(self._h, int(field), *ptrs), self._h)
+        if field != abi.HXG_FIELD_CRE:
+            out = [a.reshape(desc.nx, desc.ny, desc.nz) for a in out]
+        return out
+
+    def export_grid_file(self, field, path):
+        """Write a slot in the reference's binary grid format
+        (hxg_export_grid_file, Grid_*::export_grid)."""
+        _lib.check(self._lib.hxg_export_grid_file(self._h, int(field), os.fsencode(path)),
+                   self._h)
+
+    def generate_brnd_es(self, desc, params, observer, seed):
+        """Brnd_es::write_grid on the device into the BRND slot
+        (hxg_generate_brnd_es); the anisotropy follows the regular field of
+        the models set on this handle."""
+        obs = (C.c_double * 3)(*observer)
+        _lib.check(self._lib.hxg_generate_brnd_es(self._h, C.byref(desc), C.byref(params), obs,
+                                                  C.c_uint64(seed)), self._h)
+
+    def generate_ternd_dft(self, desc, params, observer, seed):
+        """TErnd_dft::write_grid on the device into the TERND slot."""
+        obs = (C.c_double * 3)(*observer)
+        _lib.check(self._lib.hxg_generate_ternd_dft(self._h, C.byref(desc), C.byref(params),
+                                                    obs, C.c_uint64(seed)), self._h)
+
     def set_mask(self, nside, mask):
         m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
         _lib.check(self._lib.hxg_set_mask(self._h, int(nside), _lib.dptr(m)), self._h)

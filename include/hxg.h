@@ -150,6 +150,11 @@ typedef struct {                                                   /* param.h:19
       t6_detlb2, t6_wlb2, t6_hlb2, t6_thetalb2;
   double t7_nli, t7_rli, t7_wli, t7_detthetali, t7_thetali;
 } hxg_tereg_ymw16_t;
+/* Random-field generator parameters, as Param holds them after parsing
+ * (source/param/param.cc:366-374, 693-697): rms in G for B (the n_e rms in
+ * cm^-3), k0/k1 in 1/kpc, r0/z0 in cm.                                     */
+typedef struct { double rms, k0, k1, a0, a1, rho, r0, z0; } hxg_brnd_es_t; /* param.h:167-173 */
+typedef struct { double rms, k0, a0, r0, z0; } hxg_ternd_dft_t;            /* param.h:216-221 */
 typedef struct { double alpha, beta, theta, r0, z0, E0, j0; } hxg_cre_ana_t; /* param.h:225-229 */
 typedef struct { double alpha, r0, E0, j0; } hxg_cre_unif_t;                 /* param.h:231-235 */
 
@@ -221,7 +226,6 @@ int hxg_set_models(hxg_handle *h, const hxg_models_t *m);
  * library keeps its own device copy (FP64 and/or FP32 per precision).     */
 int hxg_upload_grid(hxg_handle *h, int field, const hxg_grid_desc_t *g,
                     const double *c0, const double *c1, const double *c2);
-/* Same, from device-resident FP64 SoA arrays (no host copy).              */
 /* Load a grid straight from the reference's binary grid file
  * (Grid_*::import_grid, source/grid/grid_breg.cc:48-66 and its tereg /
  * brnd / ternd / cre twins): raw native-endian FP64, the B slots with
@@ -232,9 +236,42 @@ int hxg_upload_grid(hxg_handle *h, int field, const hxg_grid_desc_t *g,
  * the descriptor is rejected (HXG_ERR_INVALID).  Synchronous.              */
 int hxg_upload_grid_file(hxg_handle *h, int field, const hxg_grid_desc_t *g,
                          const char *path);
+/* Same, from device-resident FP64 SoA arrays (no host copy).              */
 int hxg_upload_grid_device(hxg_handle *h, int field, const hxg_grid_desc_t *g,
                            const double *d_c0, const double *d_c1,
                            const double *d_c2);
+/* Copy a slot's FP64 SoA arrays (c0,c1,c2 as in hxg_upload_grid; c1,c2
+ * ignored for scalar slots) back to host memory: the Grid_* member arrays
+ * the reference holds (include/grid.h:63,94,117,144,167).  Synchronous.  */
+int hxg_download_grid(hxg_handle *h, int field, double *c0, double *c1, double *c2);
+/* Write a slot in the reference's binary grid format: Grid_*::export_grid
+ * (source/grid/grid_brnd.cc:57-73 and its breg / tereg / ternd / cre twins;
+ * the B slots with (bx, by, bz) interleaved per voxel).  Interleaved on the
+ * device, written from pinned double buffers.  Synchronous.               */
+int hxg_export_grid_file(hxg_handle *h, int field, const char *path);
+
+/* ---- random-field generators: fill a grid slot on the device, as the
+ * reference's Pipeline::assemble_brnd / assemble_ternd do with
+ * build_permission (source/pipeline/pipeline.cc:87-140).  The slot is then
+ * read like an uploaded grid.  FFTs are cuFFT double-complex transforms;
+ * the Gaussian deviates of k-space cell c (x-major index, z fastest) are
+ * Philox4x32-10 keyed by seed with counter {c, c >> 32, b, 0x52464721}
+ * (b = 0, 1), through Box-Muller, so a field depends on the seed alone.
+ * seed 0 draws a seed from the clock, as toolkit::random_seed(0) does
+ * (include/toolkit.h:122-140).  observer = Param::observer (cm), used by
+ * the spatial profile.  Synchronous.
+ *
+ * Brnd_es::write_grid (source/field/b/brnd_es.cc:76-308) into the BRND
+ * slot: the anisotropy direction is the regular field of the handle's
+ * models (hxg_set_models first): HXG_BREG_GRID reads the uploaded BREG
+ * slot trilinearly (breg.cc:28-97), analytic models are evaluated.       */
+int hxg_generate_brnd_es(hxg_handle *h, const hxg_grid_desc_t *g, const hxg_brnd_es_t *p,
+                         const double observer[3], uint64_t seed);
+/* TErnd_dft::write_grid (source/field/te/ternd_dft.cc:35-128) into the
+ * TERND slot.                                                               */
+int hxg_generate_ternd_dft(hxg_handle *h, const hxg_grid_desc_t *g,
+                           const hxg_ternd_dft_t *p, const double observer[3],
+                           uint64_t seed);
 
 /* ---- mask: Grid_obs::mask_map (source/grid/grid_obs.cc:44-50) and its
  * per-shell Hampisk::duplicate (include/hamsk.h:55-103).  A pixel is

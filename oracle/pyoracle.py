@@ -155,6 +155,17 @@ class Oracle(_Lib):
     def temp_convert(self, t, freq):
         return self.lib.hxo_temp_convert(C.c_double(t), C.c_double(freq))
 
+    def breg_field(self, models, observer, pos):
+        """Analytic regular field (hxo_breg_field) at (n, 3) positions."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros((len(pos), 3))
+        obs = (C.c_double * 3)(*observer)
+        o = (C.c_double * 3)()
+        for i in range(len(pos)):
+            self.lib.hxo_breg_field(C.byref(models), obs, (C.c_double * 3)(*pos[i]), o)
+            out[i] = o[:]
+        return out
+
     def sync_emissivity(self, models, observer, freq, pos, b_per):
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
         jt, jp = np.zeros(len(pos)), np.zeros(len(pos))
@@ -272,3 +283,28 @@ class Reference(_Lib):
         if st != 0:
             raise RuntimeError(f"reference sync_emissivity failed: {st}")
         return jt, jp
+
+    def generate_brnd_es(self, models, grids, observer, desc, p, seed):
+        """Brnd_es::write_grid on the reference with the cell-indexed
+        deviates of the device generator; returns (bx, by, bz) as
+        (nx, ny, nz) arrays."""
+        g, keep = make_grids(grids)
+        n = desc.nx * desc.ny * desc.nz
+        out = [np.zeros(n) for _ in range(3)]
+        obs = (C.c_double * 3)(*observer)
+        st = self.lib.hxref_generate_brnd_es(C.byref(models), C.byref(g), obs, C.byref(desc),
+                                             C.byref(p), C.c_uint64(seed), *(_ptr(a) for a in out))
+        if st != 0:
+            raise RuntimeError(f"reference Brnd_es failed: {st}")
+        return [a.reshape(desc.nx, desc.ny, desc.nz) for a in out]
+
+    def generate_ternd_dft(self, observer, desc, p, seed):
+        """TErnd_dft::write_grid on the reference (cell-indexed deviates)."""
+        n = desc.nx * desc.ny * desc.nz
+        out = np.zeros(n)
+        obs = (C.c_double * 3)(*observer)
+        st = self.lib.hxref_generate_ternd_dft(obs, C.byref(desc), C.byref(p), C.c_uint64(seed),
+                                               _ptr(out))
+        if st != 0:
+            raise RuntimeError(f"reference TErnd_dft failed: {st}")
+        return out.reshape(desc.nx, desc.ny, desc.nz)

@@ -29,6 +29,7 @@
 #include <integrator.h>
 #include <param.h>
 #include <tefield.h>
+#include <gsl/gsl_rng.h>
 
 #include "hxo.h"
 
@@ -541,6 +542,80 @@ int hxref_sync_emissivity(const hxg_models_t *m, const hxo_grids_t *g,
     jt[i] = p.sync_emissivity_t(q, par.get(), f.cre.get(), f.gcre.get(), b_per[i]);
     jp[i] = p.sync_emissivity_p(q, par.get(), f.cre.get(), f.gcre.get(), b_per[i]);
   }
+  return HXG_OK;
+}
+
+/* Brnd_es::write_grid / TErnd_dft::write_grid through the reference, run on
+ * one thread with the shim's cell-indexed deviates (shim/gsl/gsl_rng.h), so
+ * that draw t is deviate t % k of k-space cell 1 + t / k: the deviates the
+ * device generators use.  The FFTs are the shim's direct-sum DFT. */
+int hxref_generate_brnd_es(const hxg_models_t *m, const hxo_grids_t *g,
+                           const double observer[3], const hxg_grid_desc_t *d,
+                           const hxg_brnd_es_t *p, uint64_t seed, double *bx,
+                           double *by, double *bz) {
+  const int threads = omp_get_max_threads();
+  omp_set_num_threads(1);
+  hxo_shim_cell_stream(4);
+  auto par = std::make_unique<Param>();
+  par->observer = Hamvec<3, ham_float>{observer[0], observer[1], observer[2]};
+  hxg_models_t mm = *m;
+  mm.brnd = HXG_BRND_NONE;
+  mm.tereg = HXG_TEREG_NONE;
+  mm.ternd = HXG_TERND_NONE;
+  mm.cre = HXG_CRE_NONE;
+  Fields f;
+  int st = build_fields(par.get(), &mm, g, &f);
+  if (st == HXG_OK) {
+    set_box(par->grid_brnd, *d);
+    par->grid_brnd.build_permission = true;
+    par->grid_brnd.read_permission = false;
+    par->brnd_seed = seed;
+    par->brnd_es.rms = p->rms;
+    par->brnd_es.k0 = p->k0;
+    par->brnd_es.k1 = p->k1;
+    par->brnd_es.a0 = p->a0;
+    par->brnd_es.a1 = p->a1;
+    par->brnd_es.rho = p->rho;
+    par->brnd_es.r0 = p->r0;
+    par->brnd_es.z0 = p->z0;
+    Grid_brnd grid(par.get());
+    Brnd_es gen;
+    gen.write_grid(par.get(), f.breg.get(), f.gbreg.get(), &grid);
+    const size_t n = par->grid_brnd.full_size;
+    std::memcpy(bx, grid.bx.get(), n * sizeof(double));
+    std::memcpy(by, grid.by.get(), n * sizeof(double));
+    std::memcpy(bz, grid.bz.get(), n * sizeof(double));
+  }
+  hxo_shim_cell_stream(0);
+  omp_set_num_threads(threads);
+  return st;
+}
+
+int hxref_generate_ternd_dft(const double observer[3], const hxg_grid_desc_t *d,
+                             const hxg_ternd_dft_t *p, uint64_t seed, double *te) {
+  const int threads = omp_get_max_threads();
+  omp_set_num_threads(1);
+  hxo_shim_cell_stream(2);
+  auto par = std::make_unique<Param>();
+  par->observer = Hamvec<3, ham_float>{observer[0], observer[1], observer[2]};
+  set_box(par->grid_ternd, *d);
+  par->grid_ternd.build_permission = true;
+  par->grid_ternd.read_permission = false;
+  // TErnd_dft seeds from brnd_seed (ternd_dft.cc:42-49)
+  par->brnd_seed = seed;
+  par->ternd_dft.rms = p->rms;
+  par->ternd_dft.k0 = p->k0;
+  par->ternd_dft.a0 = p->a0;
+  par->ternd_dft.r0 = p->r0;
+  par->ternd_dft.z0 = p->z0;
+  {
+    Grid_ternd grid(par.get());
+    TErnd_dft gen;
+    gen.write_grid(par.get(), nullptr, nullptr, &grid);
+    std::memcpy(te, grid.te.get(), par->grid_ternd.full_size * sizeof(double));
+  }
+  hxo_shim_cell_stream(0);
+  omp_set_num_threads(threads);
   return HXG_OK;
 }
 

@@ -1,7 +1,7 @@
 /* Stand-in for FFTW 3.3's fftw3.h.  On the integration path FFTW only
  * allocates buffers and creates plans (Grid_brnd/Grid_ternd::build_grid);
- * transforms run only inside the random-field generators, which the oracle
- * never calls, so fftw_execute_dft aborts. */
+ * the random-field generators run the transforms, here an unnormalised
+ * direct-sum DFT for the small grids of the tests (shim.cc). */
 #ifndef HXO_SHIM_FFTW3_H
 #define HXO_SHIM_FFTW3_H
 #include <cstddef>

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <vector>
 
 #include <fftw3.h>
 #include <gsl/gsl_randist.h>
@@ -47,16 +48,58 @@ double gsl_sf_synchrotron_2(const double x) {
   return x * std::cyl_bessel_k(2. / 3., x);
 }
 
-// ---- GSL RNG stand-in (generators only; never on the integration path) --
+// ---- GSL RNG stand-in ----------------------------------------------------
+// Default: splitmix64 uniforms, Box-Muller normals.  Cell-stream mode
+// (hxo_shim_cell_stream(k), k > 0): draw t of a generator seeded with s is
+// deviate t % k of k-space cell 1 + t / k (the generators skip cell 0), from
+// Philox4x32-10 (Salmon et al., SC 2011) keyed by s with counter
+// {cell, cell >> 32, block, 0x52464721} and Box-Muller on 53-bit uniforms:
+// the same deviates the device generators draw for that cell.
+static int g_cell_stream = 0;
+extern "C" void hxo_shim_cell_stream(int k) { g_cell_stream = k; }
+
+static void philox4x32_10(unsigned c[4], unsigned k0, unsigned k1) {
+  for (int r = 0; r < 10; ++r) {
+    const unsigned long long p0 = 0xD2511F53ull * c[0], p1 = 0xCD9E8D57ull * c[2];
+    const unsigned n0 = (unsigned)(p1 >> 32) ^ c[1] ^ k0;
+    const unsigned n2 = (unsigned)(p0 >> 32) ^ c[3] ^ k1;
+    c[1] = (unsigned)p1;
+    c[3] = (unsigned)p0;
+    c[0] = n0;
+    c[2] = n2;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+static double cell_deviate(unsigned long long seed, unsigned long long cell, int q) {
+  const int b = q / 2, pair = q % 2;
+  unsigned c[4] = {(unsigned)cell, (unsigned)(cell >> 32), (unsigned)b, 0x52464721u};
+  philox4x32_10(c, (unsigned)seed, (unsigned)(seed >> 32));
+  double u[2];
+  for (int i = 0; i < 2; ++i) {
+    const unsigned long long w = ((unsigned long long)c[2 * i] << 21) ^ (c[2 * i + 1] >> 11);
+    u[i] = ((double)(w & ((1ull << 53) - 1)) + 0.5) * (1.0 / 9007199254740992.0);
+  }
+  const double r = std::sqrt(-2. * std::log(u[0]));
+  const double a = 6.283185307179586476925 * u[1];
+  return pair == 0 ? r * std::cos(a) : r * std::sin(a);
+}
+
 static const gsl_rng_type kTaus = {1};
 const gsl_rng_type *gsl_rng_taus = &kTaus;
 gsl_rng *gsl_rng_alloc(const gsl_rng_type *) {
   gsl_rng *r = static_cast<gsl_rng *>(std::malloc(sizeof(gsl_rng)));
   r->state = 0x9E3779B97F4A7C15ULL;
+  r->seed = 0;
+  r->draws = 0;
   return r;
 }
 void gsl_rng_set(const gsl_rng *r, unsigned long int seed) {
-  const_cast<gsl_rng *>(r)->state = seed * 0x9E3779B97F4A7C15ULL + 1;
+  gsl_rng *s = const_cast<gsl_rng *>(r);
+  s->state = seed * 0x9E3779B97F4A7C15ULL + 1;
+  s->seed = seed;
+  s->draws = 0;
 }
 void gsl_rng_free(gsl_rng *r) { std::free(r); }
 double gsl_rng_uniform(const gsl_rng *r) {
@@ -68,28 +111,64 @@ double gsl_rng_uniform(const gsl_rng *r) {
   return (z >> 11) * (1.0 / 9007199254740992.0);
 }
 double gsl_ran_ugaussian(const gsl_rng *r) {
+  if (g_cell_stream > 0) {
+    gsl_rng *s = const_cast<gsl_rng *>(r);
+    const unsigned long long t = s->draws++;
+    return cell_deviate(s->seed, 1 + t / g_cell_stream, (int)(t % g_cell_stream));
+  }
   double u1 = gsl_rng_uniform(r), u2 = gsl_rng_uniform(r);
   if (u1 < 1e-300) u1 = 1e-300;
   return std::sqrt(-2. * std::log(u1)) * std::cos(6.283185307179586 * u2);
 }
 
-// ---- FFTW stand-in: allocation and plan bookkeeping only ----------------
+// ---- FFTW stand-in: unnormalised 3-D DFT by separable direct sums --------
+// FFTW's definition: out[k] = sum_j in[j] exp(sign 2 pi i j k / n) along
+// each axis, row-major (n2 fastest).  O(n) per output, for the small grids
+// the tests run.
 struct hxo_fftw_plan_s {
-  int dummy;
+  int n[3];
+  int sign;
 };
 fftw_complex *fftw_alloc_complex(std::size_t n) {
   return static_cast<fftw_complex *>(std::malloc(n * sizeof(fftw_complex)));
 }
 void fftw_free(void *p) { std::free(p); }
-fftw_plan fftw_plan_dft_3d(int, int, int, fftw_complex *, fftw_complex *, int,
+fftw_plan fftw_plan_dft_3d(int n0, int n1, int n2, fftw_complex *, fftw_complex *, int sign,
                            unsigned) {
-  return new hxo_fftw_plan_s{0};
+  return new hxo_fftw_plan_s{{n0, n1, n2}, sign};
 }
 void fftw_destroy_plan(fftw_plan p) { delete p; }
-void fftw_execute_dft(const fftw_plan, fftw_complex *, fftw_complex *) {
-  std::fprintf(stderr, "oracle build: FFTs (random-field generators) are not "
-                       "available; read field grids from files instead\n");
-  std::abort();
+void fftw_execute_dft(const fftw_plan p, fftw_complex *in, fftw_complex *out) {
+  const std::size_t n0 = p->n[0], n1 = p->n[1], n2 = p->n[2];
+  const std::size_t total = n0 * n1 * n2;
+  if (out != in)
+    for (std::size_t i = 0; i < total; ++i) out[i][0] = in[i][0], out[i][1] = in[i][1];
+  const std::size_t stride[3] = {n1 * n2, n2, 1};
+  for (int ax = 0; ax < 3; ++ax) {
+    const std::size_t n = p->n[ax];
+    std::vector<double> wr(n), wi(n), lr(n), li(n);
+    for (std::size_t m = 0; m < n; ++m) {
+      const double a = 6.283185307179586476925 * (double)m / (double)n;
+      wr[m] = std::cos(a);
+      wi[m] = p->sign * std::sin(a);
+    }
+    const std::size_t st = stride[ax];
+    for (std::size_t base = 0; base < total; ++base) {
+      if ((base / st) % n != 0) continue;  // first element of each line
+      for (std::size_t k = 0; k < n; ++k) {
+        double sr = 0., si = 0.;
+        for (std::size_t j = 0; j < n; ++j) {
+          const std::size_t m = (j * k) % n;
+          const double xr = out[base + j * st][0], xi = out[base + j * st][1];
+          sr += xr * wr[m] - xi * wi[m];
+          si += xr * wi[m] + xi * wr[m];
+        }
+        lr[k] = sr;
+        li[k] = si;
+      }
+      for (std::size_t k = 0; k < n; ++k) out[base + k * st][0] = lr[k], out[base + k * st][1] = li[k];
+    }
+  }
 }
 int fftw_init_threads(void) { return 1; }
 void fftw_plan_with_nthreads(int) {}

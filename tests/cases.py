@@ -168,3 +168,66 @@ def case_cre_grid():
     m.cre = abi.HXG_CRE_GRID
     passes = [W.make_obs([8, 16], 20.0, 0.05, freq_ghz=f) for f in (1.4, 0.408)]
     return passes, m, {abi.HXG_FIELD_CRE: (d, [np.ascontiguousarray(flux.reshape(-1))])}
+
+
+# ---- random-field generators --------------------------------------------
+
+RFG_OBSERVER = (-8.3 * U.kpc, 0.0, 0.006 * U.kpc)
+
+
+def _rfg_desc(n, box_kpc):
+    d = abi.GridDesc()
+    d.nx, d.ny, d.nz = n
+    d.x_min, d.x_max, d.y_min, d.y_max, d.z_min, d.z_max = (v * U.kpc for v in box_kpc)
+    return d
+
+
+def rfg_es(rms_muG=0.8, k0=10.0, k1=0.1, a0=1.7, a1=0.0, rho=1.0, r0_kpc=8.0, z0_kpc=1.0):
+    """Brnd_es parameters; defaults are templates/params_template.xml:239-249."""
+    p = abi.BrndEs()
+    p.rms, p.k0, p.k1, p.a0, p.a1, p.rho = rms_muG * U.muGauss, k0, k1, a0, a1, rho
+    p.r0, p.z0 = r0_kpc * U.kpc, z0_kpc * U.kpc
+    return p
+
+
+def rfg_dft(rms=1.0, k0=2.0, a0=-1.7, r0_kpc=8.0, z0_kpc=1.0):
+    """TErnd_dft parameters; defaults are templates/params_template.xml:399-406."""
+    p = abi.TerndDft()
+    p.rms, p.k0, p.a0, p.r0, p.z0 = rms, k0, a0, r0_kpc * U.kpc, z0_kpc * U.kpc
+    return p
+
+
+def case_rfg(jf12_block=None):
+    """Generator cases: (name, kind, desc, params, seed, models, grids).
+    Boxes of a few tens of kpc give k = i / L below the template's k0 of
+    the n_e spectrum, so those cases lower k0 to keep power on the grid.
+    The B cases cover an analytic field everywhere non-zero (LSA), one that
+    is zero outside 3-20 kpc (the spiral: unscaled vertices), a BREG grid
+    on a smaller box (zero outside it), and JF12 when its block is given;
+    the sizes mix odd and even axes (Nyquist planes)."""
+    A = (-20., 20., -18., 18., -4., 4.)
+    out = []
+    out.append(("ternd_a", "ternd", _rfg_desc((12, 10, 9), A), rfg_dft(k0=0.06), 12345,
+                None, None))
+    out.append(("ternd_even", "ternd", _rfg_desc((8, 8, 8), (-2., 2., -2., 2., -1., 1.)),
+                rfg_dft(rms=0.5, a0=-11. / 3., k0=0.3), 5, None, None))
+    m = W.spiral_models()
+    m.breg = abi.HXG_BREG_LSA
+    m.lsa.b0, m.lsa.psi0, m.lsa.psi1, m.lsa.chi0 = 2e-6, 27 * U.rad, 0.9 * U.rad, 25 * U.rad
+    out.append(("brnd_lsa", "brnd", _rfg_desc((12, 10, 9), A), rfg_es(rho=3.0), 777, m, None))
+    out.append(("brnd_spiral", "brnd", _rfg_desc((10, 12, 8), (-25., 25., -25., 25., -3., 3.)),
+                rfg_es(rho=0.5, a1=-0.4), 31, W.spiral_models(), None))
+    gd = _rfg_desc((9, 9, 7), (-15., 15., -14., 14., -2., 2.))
+    rng = np.random.Generator(np.random.PCG64(17))
+    gb = [rng.normal(0., 1e-6, 9 * 9 * 7) for _ in range(3)]
+    m = W.spiral_models()
+    m.breg = abi.HXG_BREG_GRID
+    out.append(("brnd_grid", "brnd", _rfg_desc((10, 8, 12), A), rfg_es(rho=2.0), 99, m,
+                {abi.HXG_FIELD_BREG: (gd, gb)}))
+    if jf12_block is not None:
+        m = W.spiral_models()
+        m.breg = abi.HXG_BREG_JF12
+        m.jf12 = jf12_block
+        out.append(("brnd_jf12", "brnd", _rfg_desc((11, 10, 8), A), rfg_es(rho=3.0), 4242, m,
+                    None))
+    return out

@@ -19,6 +19,11 @@ that holds the hammurabiX source tree; the outputs are committed).
 5. ref_cre_grid.npz -- the same for the CRE-grid emissivity on the power-law
    CRE grid of tests/cases.py:case_cre_grid (the reference built with the
    oracle's F and G, oracle/shim/shim.cc).
+6. ref_rfg.npz -- Brnd_es / TErnd_dft fields generated by the reference's
+   own generator code on the cases of tests/cases.py:case_rfg, run on one
+   thread with the shim's cell-indexed Philox deviates and its direct-sum
+   DFT (oracle/shim), i.e. the deviates the device generators draw; each
+   case's hxg_models_t block is stored beside its field.
 
 Usage: python tests/golden/make_golden.py [hammurabiX source dir]
 """
@@ -122,11 +127,26 @@ def reference_cre_grid():
     np.savez_compressed(os.path.join(HERE, "ref_cre_grid.npz"), **out)
 
 
+def reference_rfg(src):
+    ref = pyoracle.Reference()
+    blocks = _template_blocks(src)
+    out = {}
+    for name, kind, desc, p, seed, m, grids in cases.case_rfg(blocks["jf12"]):
+        if kind == "ternd":
+            out[f"{name}/te"] = ref.generate_ternd_dft(cases.RFG_OBSERVER, desc, p, seed)
+        else:
+            bx, by, bz = ref.generate_brnd_es(m, grids, cases.RFG_OBSERVER, desc, p, seed)
+            out[f"{name}/bx"], out[f"{name}/by"], out[f"{name}/bz"] = bx, by, bz
+            out[f"{name}/models"] = np.frombuffer(bytes(m), dtype=np.uint8).copy()
+    np.savez_compressed(os.path.join(HERE, "ref_rfg.npz"), **out)
+
+
 if __name__ == "__main__":
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     reference_fixtures(src)
     reference_maps()
     reference_models_ext(src)
     reference_cre_grid()
+    reference_rfg(src)
     for f in sorted(os.listdir(HERE)):
         print(f, os.path.getsize(os.path.join(HERE, f)))

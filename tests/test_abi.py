@@ -42,14 +42,16 @@ def test_struct_layouts_match_header(tmp_path):
                     ' sizeof(hxg_models_t), sizeof(hxg_obs_t), sizeof(hxg_grid_desc_t),'
                     ' offsetof(hxg_models_t, cre_unif), offsetof(hxg_obs_t, sync_freq),'
                     ' offsetof(hxg_models_t, ymw16), offsetof(hxg_grid_desc_t, E_fact),'
-                    ' sizeof(hxg_batch_entry_t), offsetof(hxg_batch_entry_t, d_us));}\n')
+                    ' sizeof(hxg_batch_entry_t), offsetof(hxg_batch_entry_t, d_us));'
+                    ' printf("%zu %zu\\n", sizeof(hxg_brnd_es_t), sizeof(hxg_ternd_dft_t));}\n')
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-o", str(exe), str(prog)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True,
                                           check=True).stdout.split()]
     want = [C.sizeof(abi.Models), C.sizeof(abi.Obs), C.sizeof(abi.GridDesc),
             abi.Models.cre_unif.offset, abi.Obs.sync_freq.offset, abi.Models.ymw16.offset,
-            abi.GridDesc.E_fact.offset, C.sizeof(abi.BatchEntry), abi.BatchEntry.d_us.offset]
+            abi.GridDesc.E_fact.offset, C.sizeof(abi.BatchEntry), abi.BatchEntry.d_us.offset,
+            C.sizeof(abi.BrndEs), C.sizeof(abi.TerndDft)]
     assert got == want
 
 
