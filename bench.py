@@ -513,7 +513,7 @@ def main():
                         f"({BYTES_PER_SAMPLE['fp32c']} B per sample); consecutive samples of a "
                         "ray re-read the same voxels from L1/L2, so DRAM traffic stays far "
                         "below it and the kernel is bound by instruction issue, not HBM",
-                "kernel": "hxg::shell_fp32c_kernel<1,true>",
+                "kernel": "hxg::shell_fp32c_kernel<1,false>",
                 "kernel_share_of_step": (kms / 1e3) / t32 if t32 > 0 else None,
                 "kernel_samples_per_s": ksamples / (kms / 1e3) if kms > 0 else None}
 

@@ -9,6 +9,7 @@
 typedef struct {
   unsigned long long state;
   unsigned long long seed, draws;
+  int cells; /* deviates per k-space cell in cell-stream mode, 0 = off */
 } gsl_rng;
 typedef struct { int id; } gsl_rng_type;
 extern const gsl_rng_type *gsl_rng_taus;
@@ -16,6 +17,9 @@ gsl_rng *gsl_rng_alloc(const gsl_rng_type *t);
 void gsl_rng_set(const gsl_rng *r, unsigned long int seed);
 void gsl_rng_free(gsl_rng *r);
 double gsl_rng_uniform(const gsl_rng *r);
-/* k deviates per k-space cell (4 for Brnd_es, 2 for TErnd_dft); 0 = off */
+/* k deviates per k-space cell (4 for Brnd_es, 2 for TErnd_dft) for every
+ * generator seeded from now on; 0 = off, then the environment variable
+ * HXO_SHIM_CELL_STREAM decides: "k" for all, or "k0,k1,..." for the 1st,
+ * 2nd, ... gsl_rng_set call of the process (the last value repeats). */
 extern "C" void hxo_shim_cell_stream(int k);
 #endif

@@ -55,8 +55,25 @@ double gsl_sf_synchrotron_2(const double x) {
 // Philox4x32-10 (Salmon et al., SC 2011) keyed by s with counter
 // {cell, cell >> 32, block, 0x52464721} and Box-Muller on 53-bit uniforms:
 // the same deviates the device generators draw for that cell.
+// The reference CLI (oracle/_ref/hamx) takes the mode from the environment:
+// HXO_SHIM_CELL_STREAM = "k" or "k0,k1,..." per gsl_rng_set call in order
+// (the Pipeline runs TErnd_dft before Brnd_es, main_std.cc:35-36).
 static int g_cell_stream = 0;
 extern "C" void hxo_shim_cell_stream(int k) { g_cell_stream = k; }
+static int cells_for_next_seed() {
+  static int calls = 0;
+  const int call = calls++;
+  if (g_cell_stream > 0) return g_cell_stream;
+  const char *e = std::getenv("HXO_SHIM_CELL_STREAM");
+  if (!e) return 0;
+  int k = 0;
+  for (int i = 0; i <= call && *e; ++i) {
+    k = std::atoi(e);
+    while (*e && *e != ',') ++e;
+    if (*e == ',') ++e;
+  }
+  return k;
+}
 
 static void philox4x32_10(unsigned c[4], unsigned k0, unsigned k1) {
   for (int r = 0; r < 10; ++r) {
@@ -93,6 +110,7 @@ gsl_rng *gsl_rng_alloc(const gsl_rng_type *) {
   r->state = 0x9E3779B97F4A7C15ULL;
   r->seed = 0;
   r->draws = 0;
+  r->cells = 0;
   return r;
 }
 void gsl_rng_set(const gsl_rng *r, unsigned long int seed) {
@@ -100,6 +118,7 @@ void gsl_rng_set(const gsl_rng *r, unsigned long int seed) {
   s->state = seed * 0x9E3779B97F4A7C15ULL + 1;
   s->seed = seed;
   s->draws = 0;
+  s->cells = cells_for_next_seed();
 }
 void gsl_rng_free(gsl_rng *r) { std::free(r); }
 double gsl_rng_uniform(const gsl_rng *r) {
@@ -111,10 +130,11 @@ double gsl_rng_uniform(const gsl_rng *r) {
   return (z >> 11) * (1.0 / 9007199254740992.0);
 }
 double gsl_ran_ugaussian(const gsl_rng *r) {
-  if (g_cell_stream > 0) {
+  const int k = r->cells;
+  if (k > 0) {
     gsl_rng *s = const_cast<gsl_rng *>(r);
     const unsigned long long t = s->draws++;
-    return cell_deviate(s->seed, 1 + t / g_cell_stream, (int)(t % g_cell_stream));
+    return cell_deviate(s->seed, 1 + t / k, (int)(t % k));
   }
   double u1 = gsl_rng_uniform(r), u2 = gsl_rng_uniform(r);
   if (u1 < 1e-300) u1 = 1e-300;
