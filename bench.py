@@ -138,8 +138,8 @@ def setup_dist(args, gpu=True):
     if ws > 1 and gpu:
         import torch
         torch.cuda.set_device(local)
-        return replicas.init("nccl", 600, torch.device("cuda", local))
-    return replicas.init("gloo", 600) if ws > 1 else (ws, rank, local)
+        return replicas.init("nccl", 120, torch.device("cuda", local))
+    return replicas.init("gloo", 120) if ws > 1 else (ws, rank, local)
 
 
 def make_passes(wl, nside_shells=None):
@@ -336,6 +336,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=2)
     ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--mode", default="shard", choices=["shard", "replicas"],
+                    help="N > 1: split each pass's shell pixels across the ranks with one FD "
+                         "all-reduce per shell (shard, strong scaling) or run N independent "
+                         "copies (replicas, weak scaling)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -346,8 +350,9 @@ def main():
     from hammurabix_b200 import abi, workloads as W
     from hammurabix_b200.integrator import Integrator
 
-    from hammurabix_b200 import replicas
+    from hammurabix_b200 import replicas, sharded
     ws, rank, local = setup_dist(args)
+    shard = ws > 1 and args.mode == "shard"
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     # a dedicated stream: the library launches on it and the CUDA events
@@ -378,10 +383,29 @@ def main():
         ig.upload_grid_device(abi.HXG_FIELD_TEREG, desc, f64[3:])
         return ig
 
-    def step(ig, outs):
-        for o in passes:
+    # shard mode: shell maps for the per-shell exchange, summed with NCCL on
+    # the launch stream (torch's current stream)
+    shell_tmp = None
+    if shard:
+        import torch.distributed as dist
+        nmax = max(abi.npix(n) for n in wl["nside_shells"])
+        shell_tmp = {k: torch.zeros(nmax, dtype=torch.float64, device=dev)
+                     for k in sharded.MAPS}
+
+        def reduce_sum(t):
+            dist.all_reduce(t)
+
+    def run_pass(ig, o, outs):
+        if shard:
+            sharded.write_grid_sharded(ig, o, dict(zip(sharded.MAPS, outs)), shell_tmp, rank,
+                                       ws, reduce_sum)
+        else:
             ig.write_grid_device(o, outs[0] if o.do_dm else None, outs[1] if o.do_fd else None,
                                  outs[2], outs[3], outs[4])
+
+    def step(ig, outs):
+        for o in passes:
+            run_pass(ig, o, outs)
 
     def barrier():
         torch.cuda.synchronize(dev)
@@ -413,7 +437,9 @@ def main():
     launches = ig32.launch_count() - lc0
     kms, klaunch, ksamples = ig32.get_timing()
     ig32.set_timing(False)
-    value = replicas.throughput(samples_step * args.steps, ws, t32)
+    # shard: the N ranks together did one job's steps; replicas: N jobs
+    value = (samples_step * args.steps / t32 if shard
+             else replicas.throughput(samples_step * args.steps, ws, t32))
     ms_step = t32 / args.steps * 1e3
     log(f"[rank {rank}] fp32c: {ms_step:.1f} ms/step, {value:.4g} samples/s")
 
@@ -430,7 +456,7 @@ def main():
         ig64.set_timing(False)
         ms64 = t64 / args.fp64_steps * 1e3
         fp64 = {"ms_per_step": ms64, "ms_per_map": ms64 / len(passes),
-                "samples_per_s": ws * samples_step / (ms64 / 1e3),
+                "samples_per_s": (1 if shard else ws) * samples_step / (ms64 / 1e3),
                 "kernel_samples_per_s": k64s / (k64ms / 1e3) if k64ms > 0 else None}
         # errors of the last pass (0.408 GHz, sync only) and of the first
         # pass's DM/FD: rerun pass 0 and the last pass in both forms
@@ -464,12 +490,21 @@ def main():
                        for k in keys} for _ in passes]
         ige = Integrator("fp32c", device=local)
         ige.set_models(models)
+        dev_out = outputs() if shard else None
 
         def e2e_step():
             ige.upload_grid(abi.HXG_FIELD_BRND, desc, hosts[:3])
             ige.upload_grid(abi.HXG_FIELD_TEREG, desc, hosts[3:])
             for o, po in zip(passes, pinned_out):
-                ige.write_grid(o, out=po)
+                if shard:   # the split pass on device, then the maps to pinned host memory
+                    ige.set_stream(stream.cuda_stream)
+                    run_pass(ige, o, dev_out)
+                    for k, t in zip(keys, dev_out):
+                        if (k != "dm" or o.do_dm) and (k != "fd" or o.do_fd):
+                            torch.from_numpy(po[k]).copy_(t)
+                    torch.cuda.synchronize(dev)
+                else:
+                    ige.write_grid(o, out=po)
 
         e2e_step()
         barrier()
@@ -481,7 +516,8 @@ def main():
         h2d = sum(h.nbytes for h in hosts)
         d2h = sum(8 * (abi.npix(o.nside_dm) * o.do_dm + abi.npix(o.nside_fd) * o.do_fd
                        + 3 * abi.npix(o.nside_sync)) for o in passes)
-        e2e = {"value": ws * samples_step / te, "unit": UNIT, "h2d_bytes_per_step": h2d,
+        e2e = {"value": (1 if shard else ws) * samples_step / te, "unit": UNIT,
+               "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": te * 1e3}
         ige.close()
         del pinned, hosts
@@ -529,7 +565,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32c",
+            "scaling": "strong" if shard else "weak", "vs_baseline": None, "dtype": "f32c",
             "data": "synthetic",
             "config": {"workload": f"{args.workload}: Nside "
                        f"{'/'.join(str(s) for s in wl['nside_shells'])} x "
@@ -539,7 +575,9 @@ def main():
                        "samples_per_step": samples_step, "passes_per_step": len(passes),
                        "l2": "inputs larger than L2 (grids "
                              f"{4 * 4 * n ** 3 / 1e9:.2f} GB FP32)",
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+                       "parallelism": (f"shell pixels split over {ws} GPUs, FD all-reduce "
+                                       "per shell" if shard else
+                                       f"replicas x{ws}" if ws > 1 else "1 GPU")},
             "ms_per_map": ms_step / len(passes),
             "fp64": fp64,
             "fp32c_speedup_vs_fp64": (fp64["ms_per_step"] / ms_step) if fp64 else None,

@@ -604,6 +604,8 @@ int build_launch(hxg_handle *h, const hxg_models_t &m, const hxg_obs_t &o,
   P.gc_z_min = o.gc_z_min * L;
   P.gc_z_max = o.gc_z_max * L;
   P.nside = (int)o.nside_shell[s];
+  P.shard = 0;
+  P.nshards = 1;
   P.do_dm = o.do_dm != 0;
   P.do_fd = o.do_fd != 0;
   P.do_sync = o.do_sync != 0;
@@ -1214,11 +1216,12 @@ int hxg_set_mask(hxg_handle *h, uint32_t nside, const double *mask) {
   return HXG_OK;
 }
 
-int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
-                          double *d_fd, double *d_is, double *d_qs,
-                          double *d_us) {
-  if (!h) return HXG_ERR_INVALID;
-  cudaSetDevice(h->device);
+}  // extern "C"
+
+namespace {
+
+// Checks shared by the pass entry points: obs, models, requested outputs.
+int check_pass(hxg_handle *h, const hxg_obs_t *o, bool dm, bool fd, bool sync3) {
   int st = validate_obs(h, o);
   if (st != HXG_OK) return st;
   if (!h->have_models) return fail(h, HXG_ERR_STATE, "models not set");
@@ -1226,10 +1229,115 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
     return fail(h, HXG_ERR_INVALID, "synchrotron output needs a CRE model");
   if (o->do_sync && h->models.cre == HXG_CRE_GRID && !h->slots[HXG_FIELD_CRE].present)
     return fail(h, HXG_ERR_STATE, "CRE grid model without an uploaded CRE grid");
-  if ((o->do_dm && !d_dm) || (o->do_fd && !d_fd) ||
-      (o->do_sync && (!d_is || !d_qs || !d_us)))
+  if ((o->do_dm && !dm) || (o->do_fd && !fd) || (o->do_sync && !sync3))
     return fail(h, HXG_ERR_INVALID, "an output requested by obs is NULL");
-  if ((st = build_groups(h)) != HXG_OK) return st;
+  return build_groups(h);
+}
+
+// Shell s of pass o over the pixels of shard `shard` of `nshards` (the
+// 32-pixel NESTED blocks b with b % nshards == shard) into the shell maps tmp (radial_integration for every pixel of the shell,
+// integrator.cc:60-100); fdmap = the accumulated FD output of the inner
+// shells, or null.
+int run_shell(hxg_handle *h, const hxg_obs_t &o, uint32_t s, const ExtModels *ext_dev,
+              const double *fdmap, double *const tmp[5], uint32_t shard, uint32_t nshards,
+              bool checkpoint) {
+  const bool fp32 = h->precision == HXG_FP32C;
+  ShellLaunch P;
+  uint64_t step;
+  int st = build_launch(h, h->models, o, s, P, step);
+  if (st != HXG_OK) return st;
+  P.ext = ext_dev;
+  // inner-shell Faraday depth: the accumulated FD output map when it is
+  // requested, otherwise an all-zero map (integrator.cc:78-86, 130-132)
+  P.fdmap = o.do_fd ? fdmap : nullptr;
+  P.nside_fdmap = o.do_fd ? (int)o.nside_fd : 0;
+  P.mask = nullptr;
+  if (o.do_mask) {
+    const unsigned char *dm = nullptr;
+    if ((st = device_mask(h, o.nside_shell[s], &dm)) != HXG_OK) return st;
+    P.mask = dm;
+  }
+  for (int k = 0; k < 5; ++k) P.out[k] = tmp[k];
+  const uint64_t npix = npix_of(o.nside_shell[s]);
+  P.shard = shard;
+  P.nshards = nshards;
+  // pixels of this shard, counted in whole blocks (the kernel drops the
+  // ones past npix)
+  const uint64_t nblk = (npix + 31) / 32;
+  const uint64_t local = nshards == 1 ? npix : (nblk + nshards - 1 - shard) / nshards * 32;
+  const int C = choose_chunks(h, local, step);
+  P.chunks = C;
+  P.log2_chunks = hpx_ilog2((uint64_t)C);
+  if (checkpoint) {
+    if (h->ck.size() < o.total_shell) {
+      h->ck.resize(o.total_shell);
+      h->ck_inner.resize(o.total_shell);
+      h->ck_chunks.resize(o.total_shell);
+    }
+    if ((st = ensure(h, h->ck[s], npix * C * 3 * sizeof(double))) != HXG_OK) return st;
+    if ((st = ensure(h, h->ck_inner[s], npix * sizeof(double))) != HXG_OK) return st;
+    HXG_CK(cudaMemsetAsync(h->ck_inner[s].p, 0, npix * sizeof(double), h->stream));
+    P.ck = static_cast<double *>(h->ck[s].p);
+    P.ck_inner = static_cast<double *>(h->ck_inner[s].p);
+    h->ck_chunks[s] = C;
+  }
+  if (local == 0) return HXG_OK;
+  const uint64_t warps = (local + (32 / C) - 1) / (32 / C);
+  const unsigned threads = 256;
+  const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (h->timing) {
+    HXG_CK(cudaEventCreate(&e0));
+    HXG_CK(cudaEventCreate(&e1));
+    HXG_CK(cudaEventRecord(e0, h->stream));
+  }
+  HXG_CK(launch_shell(h->stream, fp32, P, blocks, threads));
+  ++h->launch_count;
+  if (h->timing) {
+    HXG_CK(cudaEventRecord(e1, h->stream));
+    h->events.emplace_back(e0, e1);
+    h->event_samples.push_back((int64_t)(std::min(local, npix) * step));
+  }
+  return HXG_OK;
+}
+
+// Accumulate the shell maps of shell s into the pass outputs
+// (Hampix::accumulate, integrator.cc:121-132).
+int merge_shell(hxg_handle *h, const hxg_obs_t &o, uint32_t s, const double *const tmp[5],
+                double *d_dm, double *d_fd, double *d_is, double *d_qs, double *d_us) {
+  const int ns = (int)o.nside_shell[s];
+  if (o.do_dm) {
+    double *d[1] = {d_dm};
+    const double *sr[1] = {tmp[0]};
+    HXG_CK(launch_accumulate(h->stream, (int)o.nside_dm, ns, 1, d, sr));
+    ++h->launch_count;
+  }
+  if (o.do_sync) {
+    double *d[3] = {d_is, d_qs, d_us};
+    const double *sr[3] = {tmp[2], tmp[3], tmp[4]};
+    HXG_CK(launch_accumulate(h->stream, (int)o.nside_sync, ns, 3, d, sr));
+    ++h->launch_count;
+  }
+  if (o.do_fd) {
+    double *d[1] = {d_fd};
+    const double *sr[1] = {tmp[1]};
+    HXG_CK(launch_accumulate(h->stream, (int)o.nside_fd, ns, 1, d, sr));
+    ++h->launch_count;
+  }
+  return HXG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
+                          double *d_fd, double *d_is, double *d_qs,
+                          double *d_us) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  int st = check_pass(h, o, d_dm, d_fd, d_is && d_qs && d_us);
+  if (st != HXG_OK) return st;
   const bool fp32 = h->precision == HXG_FP32C;
   uint32_t max_nside = 0;
   for (uint32_t s = 0; s < o->total_shell; ++s)
@@ -1250,77 +1358,13 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
   }
   const ExtModels *ext_dev = nullptr;
   if ((st = upload_ext(h, h->models, o->sync_freq, &ext_dev)) != HXG_OK) return st;
+  const bool ck = h->checkpoint && !fp32;
   for (uint32_t s = 0; s < o->total_shell; ++s) {
-    ShellLaunch P;
-    uint64_t step;
-    if ((st = build_launch(h, h->models, *o, s, P, step)) != HXG_OK) return st;
-    P.ext = ext_dev;
-    // inner-shell Faraday depth: the accumulated FD output map when it is
-    // requested, otherwise an all-zero map (integrator.cc:78-86, 130-132)
-    P.fdmap = o->do_fd ? d_fd : nullptr;
-    P.nside_fdmap = o->do_fd ? (int)o->nside_fd : 0;
-    P.mask = nullptr;
-    if (o->do_mask) {
-      const unsigned char *dm = nullptr;
-      if ((st = device_mask(h, o->nside_shell[s], &dm)) != HXG_OK) return st;
-      P.mask = dm;
-    }
-    for (int k = 0; k < 5; ++k) P.out[k] = tmp[k];
-    const uint64_t npix = npix_of(o->nside_shell[s]);
-    const int C = choose_chunks(h, npix, step);
-    P.chunks = C;
-    P.log2_chunks = hpx_ilog2((uint64_t)C);
-    if (h->checkpoint && !fp32) {
-      if (h->ck.size() < o->total_shell) {
-        h->ck.resize(o->total_shell);
-        h->ck_inner.resize(o->total_shell);
-        h->ck_chunks.resize(o->total_shell);
-      }
-      if ((st = ensure(h, h->ck[s], npix * C * 3 * sizeof(double))) != HXG_OK) return st;
-      if ((st = ensure(h, h->ck_inner[s], npix * sizeof(double))) != HXG_OK) return st;
-      HXG_CK(cudaMemsetAsync(h->ck_inner[s].p, 0, npix * sizeof(double), h->stream));
-      P.ck = static_cast<double *>(h->ck[s].p);
-      P.ck_inner = static_cast<double *>(h->ck_inner[s].p);
-      h->ck_chunks[s] = C;
-    }
-    const uint64_t warps = (npix + (32 / C) - 1) / (32 / C);
-    const unsigned threads = 256;
-    const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (h->timing) {
-      HXG_CK(cudaEventCreate(&e0));
-      HXG_CK(cudaEventCreate(&e1));
-      HXG_CK(cudaEventRecord(e0, h->stream));
-    }
-    HXG_CK(launch_shell(h->stream, fp32, P, blocks, threads));
-    ++h->launch_count;
-    if (h->timing) {
-      HXG_CK(cudaEventRecord(e1, h->stream));
-      h->events.emplace_back(e0, e1);
-      h->event_samples.push_back((int64_t)(npix * step));
-    }
-    // accumulate the shell maps into the outputs (integrator.cc:121-132)
-    const int ns = (int)o->nside_shell[s];
-    if (o->do_dm) {
-      double *d[1] = {d_dm};
-      const double *sr[1] = {tmp[0]};
-      HXG_CK(launch_accumulate(h->stream, (int)o->nside_dm, ns, 1, d, sr));
-      ++h->launch_count;
-    }
-    if (o->do_sync) {
-      double *d[3] = {d_is, d_qs, d_us};
-      const double *sr[3] = {tmp[2], tmp[3], tmp[4]};
-      HXG_CK(launch_accumulate(h->stream, (int)o->nside_sync, ns, 3, d, sr));
-      ++h->launch_count;
-    }
-    if (o->do_fd) {
-      double *d[1] = {d_fd};
-      const double *sr[1] = {tmp[1]};
-      HXG_CK(launch_accumulate(h->stream, (int)o->nside_fd, ns, 1, d, sr));
-      ++h->launch_count;
-    }
+    st = run_shell(h, *o, s, ext_dev, d_fd, tmp, 0, 1, ck);
+    if (st != HXG_OK) return st;
+    if ((st = merge_shell(h, *o, s, tmp, d_dm, d_fd, d_is, d_qs, d_us)) != HXG_OK) return st;
   }
-  if (h->checkpoint && !fp32) {
+  if (ck) {
     h->ck_valid = true;
     h->ck_obs = *o;
     h->ck_models = h->models;
@@ -1328,6 +1372,48 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
     h->ck_valid = false;
   }
   return HXG_OK;
+}
+
+int hxg_shell_integrate_device(hxg_handle *h, const hxg_obs_t *o, uint32_t shell,
+                               uint32_t shard, uint32_t nshards, const double *d_fd,
+                               double *d_tmp_dm, double *d_tmp_fd, double *d_tmp_is,
+                               double *d_tmp_qs, double *d_tmp_us) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  if (!o || shell >= o->total_shell || nshards == 0 || shard >= nshards)
+    return fail(h, HXG_ERR_INVALID, "bad shell %u or shard %u of %u", shell, shard, nshards);
+  const bool sync3 = d_tmp_is && d_tmp_qs && d_tmp_us;
+  int st = check_pass(h, o, d_tmp_dm, d_tmp_fd && (d_fd || !o->do_fd), sync3);
+  if (st != HXG_OK) return st;
+  if ((o->do_fd || o->do_sync) && !d_tmp_fd)
+    return fail(h, HXG_ERR_INVALID, "the shell FD map is written whenever FD or sync is on");
+  const uint64_t npix = npix_of(o->nside_shell[shell]);
+  double *tmp[5] = {d_tmp_dm, d_tmp_fd, d_tmp_is, d_tmp_qs, d_tmp_us};
+  if (nshards > 1) {  // pixels of other shards stay zero: shard maps add up
+    for (int k = 0; k < 5; ++k)
+      if (tmp[k]) HXG_CK(cudaMemsetAsync(tmp[k], 0, npix * sizeof(double), h->stream));
+  }
+  const ExtModels *ext_dev = nullptr;
+  if ((st = upload_ext(h, h->models, o->sync_freq, &ext_dev)) != HXG_OK) return st;
+  h->ck_valid = false;
+  return run_shell(h, *o, shell, ext_dev, d_fd, tmp, shard, nshards, false);
+}
+
+int hxg_shell_merge_device(hxg_handle *h, const hxg_obs_t *o, uint32_t shell,
+                           const double *d_tmp_dm, const double *d_tmp_fd,
+                           const double *d_tmp_is, const double *d_tmp_qs,
+                           const double *d_tmp_us, double *d_dm, double *d_fd,
+                           double *d_is, double *d_qs, double *d_us) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  if (!o || shell >= o->total_shell) return fail(h, HXG_ERR_INVALID, "bad shell %u", shell);
+  int st = validate_obs(h, o);
+  if (st != HXG_OK) return st;
+  if ((o->do_dm && (!d_dm || !d_tmp_dm)) || (o->do_fd && (!d_fd || !d_tmp_fd)) ||
+      (o->do_sync && (!d_is || !d_qs || !d_us || !d_tmp_is || !d_tmp_qs || !d_tmp_us)))
+    return fail(h, HXG_ERR_INVALID, "a map requested by obs is NULL");
+  const double *tmp[5] = {d_tmp_dm, d_tmp_fd, d_tmp_is, d_tmp_qs, d_tmp_us};
+  return merge_shell(h, *o, shell, tmp, d_dm, d_fd, d_is, d_qs, d_us);
 }
 
 int hxg_set_checkpointing(hxg_handle *h, int enable) {

@@ -139,7 +139,7 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw,
   const int c = lane & (C - 1);
   const Hpx h = hpx_make((uint64_t)P.nside);
   const unsigned long long nest =
-      (unsigned long long)gw * (32 >> P.log2_chunks) + seg;
+      shard_nest(P, (unsigned long long)gw * (32 >> P.log2_chunks) + seg);
   const bool valid = nest < h.npix;
   uint64_t ring = 0;
   bool live = false;

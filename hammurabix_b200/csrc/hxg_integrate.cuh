@@ -34,6 +34,10 @@ struct ShellLaunch {
   long long step;            // samples per ray (integrator.cc:237-240)
   double gc_r_min, gc_r_max, gc_z_min, gc_z_max;
   int nside, chunks, log2_chunks;
+  // shard `shard` of `nshards` of the shell: the 32-pixel NESTED blocks b
+  // with b % nshards == shard (interleaved over the sky, so that the shards
+  // see the same mix of ray lengths); 0 of 1 for the whole shell
+  unsigned shard, nshards;
   int do_dm, do_fd, do_sync;
   const double *fdmap;       // accumulated FD map of inner shells (or null)
   int nside_fdmap;
@@ -66,6 +70,14 @@ struct ShellLaunch {
   FastModels fast;  // FP32C only
   const ExtModels *ext;  // Jaffe / JF12 / YMW16 blocks (device), or null
 };
+
+// NESTED index of the shard's local pixel `local`: local pixels run through
+// the shard's 32-pixel blocks in order.
+__device__ __forceinline__ unsigned long long shard_nest(const ShellLaunch &P,
+                                                         unsigned long long local) {
+  if (P.nshards == 1) return local;
+  return (((local >> 5) * P.nshards + P.shard) << 5) + (local & 31);
+}
 
 // Sample window [lo, hi) of one ray: the samples that can pass the
 // spherical |pos| <= r_max and vertical z_min <= z <= z_max cuts
@@ -184,7 +196,7 @@ __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
   const int c = lane & (C - 1);
   const Hpx h = hpx_make((uint64_t)P.nside);
   const unsigned long long nest =
-      (unsigned long long)gw * (32 >> P.log2_chunks) + seg;
+      shard_nest(P, (unsigned long long)gw * (32 >> P.log2_chunks) + seg);
   const bool valid = nest < h.npix;
   uint64_t ring = 0;
   bool live = false;

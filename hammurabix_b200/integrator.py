@@ -137,6 +137,25 @@ class Integrator:
     def sync(self):
         _lib.check(self._lib.hxg_sync(self._h), self._h)
 
+    # ---- one shell over a shard of its pixels ---------------------------------
+    def shell_integrate_device(self, obs, shell, shard, nshards, fd, tmp):
+        """Shell `shell` for the pixels of shard `shard` of `nshards` into the
+        shell maps tmp = [dm, fd, is, qs, us] (torch CUDA float64 tensors of
+        at least 12 nside_shell^2 elements, or None where obs needs none);
+        fd = the accumulated FD output (hxg_shell_integrate_device)."""
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        _lib.check(self._lib.hxg_shell_integrate_device(
+            self._h, C.byref(obs), int(shell), int(shard), int(nshards), ptr(fd),
+            *(ptr(t) for t in tmp)), self._h)
+
+    def shell_merge_device(self, obs, shell, tmp, outs):
+        """Accumulate shell maps tmp into the pass outputs outs = [dm, fd, is,
+        qs, us] (hxg_shell_merge_device)."""
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        _lib.check(self._lib.hxg_shell_merge_device(
+            self._h, C.byref(obs), int(shell), *(ptr(t) for t in tmp),
+            *(ptr(t) for t in outs)), self._h)
+
     # ---- adjoint -----------------------------------------------------------
     def set_checkpointing(self, enable=True):
         """Store per-shell checkpoints in write_grid_device for adjoint()."""

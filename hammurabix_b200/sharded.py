@@ -1,0 +1,60 @@
+"""One frequency pass split across the ranks of a process group by shell
+pixels: the multi-GPU form of Integrator::write_grid
+(source/integrator/integrator.cc:23-134).
+
+The pixels of a shell are independent; the only exchange is the Faraday
+depth of the inner shells, which every pixel of the next shell reads from the
+accumulated FD map (integrator.cc:78-86).  So, per shell, each rank integrates
+its shard of the shell's NESTED pixels (zero elsewhere), the shell FD maps
+are summed over the ranks (an all-reduce of one map of 12 nside_shell^2
+doubles; the shards are disjoint, so the sum is the full map), and every rank
+merges the complete FD map into its FD output, which is then identical on
+all ranks.  The DM and Stokes maps are merged from each rank's partial shell
+maps (the merge is linear) and summed over the ranks once at the end.  Every
+rank issues the same collectives in the same order.
+"""
+from . import abi
+
+MAPS = ("dm", "fd", "is", "qs", "us")
+
+
+def requested(obs):
+    """Which of MAPS the pass writes."""
+    return {"dm": bool(obs.do_dm), "fd": bool(obs.do_fd), "is": bool(obs.do_sync),
+            "qs": bool(obs.do_sync), "us": bool(obs.do_sync)}
+
+
+def shell_maps_needed(obs):
+    """Which shell maps the kernel writes (the FD shell map whenever FD or
+    sync is on)."""
+    r = requested(obs)
+    r["fd"] = bool(obs.do_fd or obs.do_sync)
+    return r
+
+
+def write_grid_sharded(integ, obs, outs, tmp, rank, world, reduce_sum):
+    """One pass on this rank.
+
+    integ: an Integrator whose stream (Integrator.set_stream) is the caller's
+    current torch stream, a non-null one: the zeroing and the reductions run
+    there, between the library's launches;
+    outs: dict of the pass outputs (device tensors, the requested ones);
+    tmp: dict of shell-map buffers of 12 max(nside_shell)^2 doubles;
+    reduce_sum(t): in-place sum of t over the ranks, in stream order."""
+    req, need = requested(obs), shell_maps_needed(obs)
+    for k in MAPS:
+        if req[k]:
+            outs[k].zero_()
+    out_list = [outs[k] if req[k] else None for k in MAPS]
+    for s in range(obs.total_shell):
+        n = abi.npix(obs.nside_shell[s])
+        views = [tmp[k][:n] if need[k] else None for k in MAPS]
+        integ.shell_integrate_device(obs, s, rank, world, outs["fd"] if req["fd"] else None,
+                                     views)
+        if world > 1 and req["fd"]:
+            reduce_sum(views[1])
+        integ.shell_merge_device(obs, s, views, out_list)
+    if world > 1:
+        for k in ("dm", "is", "qs", "us"):
+            if req[k]:
+                reduce_sum(outs[k])

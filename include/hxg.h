@@ -293,6 +293,37 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *obs, double *d_dm,
 /* Wait for the handle's stream; returns the first asynchronous error.     */
 int hxg_sync(hxg_handle *h);
 
+/* ---- one shell at a time, over a shard of its pixels ---------------------
+ * The two halves of one iteration of write_grid's shell loop
+ * (integrator.cc:56-133), for callers that split a pass across GPUs: the
+ * pixels of a shell are independent, and the only exchange is the
+ * accumulated FD map, which the next shell reads for its inner-shell Faraday
+ * depth (integrator.cc:78-86).
+ *
+ * hxg_shell_integrate_device: radial integration of shell `shell` for the
+ * pixels of shard `shard` of `nshards` (the 32-pixel NESTED blocks b with
+ * b mod nshards == shard: interleaved over the sky, so every shard gets the
+ * same mix of ray lengths) into the caller's shell maps at
+ * nside_shell[shell] (RING; d_tmp_fd is written whenever FD or sync is on).
+ * With nshards > 1 the maps are zero outside the shard, so the shard maps of
+ * all shards add up to the shell's maps.  d_fd = the accumulated FD output
+ * of the inner shells, complete over all pixels (read when obs->do_fd).
+ * hxg_shell_merge_device: Hampix::accumulate of the shell maps into the
+ * pass outputs (integrator.cc:121-132); the caller zeroes the outputs before
+ * shell 0.  A pass split this way over shards: for each shell, integrate,
+ * sum the shell FD maps over the shards, merge; at the end sum the DM, I, Q,
+ * U outputs over the shards.  Both calls are asynchronous on the handle's
+ * stream.  No counterpart in the reference (its shell loop is internal).  */
+int hxg_shell_integrate_device(hxg_handle *h, const hxg_obs_t *obs, uint32_t shell,
+                               uint32_t shard, uint32_t nshards, const double *d_fd,
+                               double *d_tmp_dm, double *d_tmp_fd, double *d_tmp_is,
+                               double *d_tmp_qs, double *d_tmp_us);
+int hxg_shell_merge_device(hxg_handle *h, const hxg_obs_t *obs, uint32_t shell,
+                           const double *d_tmp_dm, const double *d_tmp_fd,
+                           const double *d_tmp_is, const double *d_tmp_qs,
+                           const double *d_tmp_us, double *d_dm, double *d_fd,
+                           double *d_is, double *d_qs, double *d_us);
+
 /* ---- adjoint (gradients of a scalar loss of the maps) -------------------
  * Reverse mode of hxg_write_grid_device (FP64 form).  With checkpointing
  * on, every forward call stores per shell the chunk Faraday depths and

@@ -1,0 +1,180 @@
+"""A pass split across ranks by shell pixels (hammurabix_b200.sharded and
+hxg_shell_integrate_device / hxg_shell_merge_device).
+
+CPU (gloo, 2 ranks): the exchange logic with a stand-in integrator that
+keeps the library's contract (shell maps zero outside the shard, a shell's
+values depend on the accumulated FD map of the inner shells, a linear
+merge): both ranks end with the single-process outputs.
+
+GPU (one device): the shards of a pass emulated one after another in one
+process -- each shard's shell maps summed the way the all-reduce sums them --
+against the unsplit hxg_write_grid_device: to rounding in FP64 (a shard has
+fewer pixels, so it may split each ray over more lanes, which regroups the
+sums) and to the FP32C tolerance.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+import torch.multiprocessing as mp  # noqa: E402
+
+from conftest import rel_err  # noqa: E402
+from hammurabix_b200 import abi, sharded, workloads as W  # noqa: E402
+
+
+def _owned(npix, r, n):
+    """NESTED pixels of shard r of n: the 32-pixel blocks b with b % n == r
+    (the library's shard_nest, written out)."""
+    nest = np.arange(npix)
+    return (nest // 32) % n == r
+
+
+class FakeIntegrator:
+    """Per-shell stand-in with the library's sharding contract."""
+
+    def shell_integrate_device(self, obs, s, shard, nshards, fd, tmp):
+        n = abi.npix(obs.nside_shell[s])
+        own = torch.from_numpy(_owned(n, shard, nshards))
+        inner = float(fd.sum()) if fd is not None else 0.0   # needs the complete FD map
+        base = 1.0 + s + 0.01 * torch.arange(n, dtype=torch.float64)
+        for k, t in enumerate(tmp):
+            if t is None:
+                continue
+            t.zero_()
+            t[own] = (k + 1) * base[own] + 1e-3 * inner
+
+    def shell_merge_device(self, obs, s, tmp, outs):
+        for t, o in zip(tmp, outs):
+            if t is None or o is None:
+                continue
+            g = torch.Generator().manual_seed(len(o) * 7919 + len(t))
+            o += torch.rand(len(o), len(t), generator=g, dtype=torch.float64) @ t
+
+
+def _obs():
+    return W.make_obs([4, 8, 8], 20.0, 0.1, freq_ghz=1.4)
+
+
+def _run(world, rank, reduce_sum):
+    o = _obs()
+    out_n = abi.npix(8)
+    outs = {k: torch.zeros(out_n, dtype=torch.float64) for k in sharded.MAPS}
+    tmp = {k: torch.zeros(out_n, dtype=torch.float64) for k in sharded.MAPS}
+    sharded.write_grid_sharded(FakeIntegrator(), o, outs, tmp, rank, world, reduce_sum)
+    return {k: v.numpy().copy() for k, v in outs.items()}
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, ws, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(ws),
+                      RANK=str(rank), LOCAL_RANK=str(rank))
+    import torch.distributed as dist
+    from hammurabix_b200 import replicas
+    w, r, _ = replicas.init("gloo", 60)
+    q.put((r, _run(w, r, lambda t: dist.all_reduce(t))))
+    replicas.finish(w)
+
+
+def test_two_gloo_ranks_reproduce_the_single_process_pass():
+    single = _run(1, 0, None)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for r in (0, 1):
+        for k in sharded.MAPS:
+            assert np.abs(single[k]).max() > 0, k
+            assert rel_err(got[r][k], single[k]) <= 1e-12, (r, k)
+
+
+def test_shards_partition_every_shell():
+    """shard_nest (hxg_integrate.cuh) maps each shard's local pixels onto its
+    blocks; over all shards every NESTED pixel is taken exactly once."""
+    for npix in (12, 48, 192, 768, 12 * 64 ** 2):
+        for n in (1, 2, 3, 8):
+            seen = np.zeros(npix, dtype=int)
+            nblk = (npix + 31) // 32
+            for r in range(n):
+                local = np.arange((nblk + n - 1 - r) // n * 32 if n > 1 else npix)
+                nest = local if n == 1 else ((local >> 5) * n + r) * 32 + (local & 31)
+                nest = nest[nest < npix]
+                assert np.all(_owned(npix, r, n)[nest])
+                seen[nest] += 1
+            assert np.all(seen == 1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32c", 1e-5)])
+@pytest.mark.parametrize("nshards", [2, 3])
+def test_emulated_shards_match_the_unsplit_pass(fields32, precision, tol, nshards):
+    from hammurabix_b200.integrator import Integrator
+    dev = torch.device("cuda", 0)
+    # one stream for the library and torch's own work on the maps (a null
+    # stream handle would leave the library on its own stream)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    bx, by, bz, ne = (torch.tensor(np.asarray(a, dtype=np.float64).reshape(-1), device=dev)
+                      for a in fields32)
+    passes = [W.make_obs([8, 16, 32], 20.0, 0.05, freq_ghz=0.408),
+              W.make_obs([8, 16, 32], 20.0, 0.05, freq_ghz=23.0, do_fd=False)]
+    with Integrator(precision) as integ:
+        integ.set_stream(stream.cuda_stream)
+        integ.set_models(W.grid_models())
+        integ.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(32), [bx, by, bz])
+        integ.upload_grid_device(abi.HXG_FIELD_TEREG, W.grid_desc(32), [ne])
+        for o in passes:
+            ndm, nfd, nsy = abi.obs_output_sizes(o)
+            z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev) if n else None
+            ref = [z(ndm), z(nfd), z(nsy), z(nsy), z(nsy)]
+            integ.write_grid_device(o, *ref)
+            req = sharded.requested(o)
+            need = sharded.shell_maps_needed(o)
+            nmax = abi.npix(max(o.nside_shell[s] for s in range(o.total_shell)))
+            # per-shard outputs; the FD output is shared (every rank holds the same)
+            outs = [[z(ndm), None, z(nsy), z(nsy), z(nsy)] for _ in range(nshards)]
+            fd = z(nfd)
+            for s in range(o.total_shell):
+                n = abi.npix(o.nside_shell[s])
+                shard_tmp = []
+                for r in range(nshards):
+                    t = [z(nmax)[:n] if need[k] else None for k in sharded.MAPS]
+                    integ.shell_integrate_device(o, s, r, nshards, fd, t)
+                    shard_tmp.append(t)
+                fd_sum = None
+                if req["fd"]:
+                    fd_sum = sum(t[1] for t in shard_tmp)       # the per-shell all-reduce
+                for r in range(nshards):
+                    t = list(shard_tmp[r])
+                    out_r = list(outs[r])
+                    if req["fd"]:
+                        # every rank merges the summed FD map; one FD output
+                        # stands for all of them (they are identical)
+                        t[1] = fd_sum
+                        out_r[1] = fd if r == 0 else z(nfd)
+                    integ.shell_merge_device(o, s, t, out_r)
+            integ.sync()
+            got = [None] * 5
+            got[1] = fd
+            for j in (0, 2, 3, 4):
+                if outs[0][j] is not None:
+                    got[j] = sum(outs[r][j] for r in range(nshards))  # the final all-reduce
+            for j, k in enumerate(sharded.MAPS):
+                if not req[k]:
+                    continue
+                a, b = got[j].cpu().numpy(), ref[j].cpu().numpy()
+                assert rel_err(a, b) <= tol, (k, rel_err(a, b))
+                assert np.abs(b).max() > 0, k
