@@ -34,10 +34,11 @@ struct ShellLaunch {
   long long step;            // samples per ray (integrator.cc:237-240)
   double gc_r_min, gc_r_max, gc_z_min, gc_z_max;
   int nside, chunks, log2_chunks;
-  // shard `shard` of `nshards` of the shell: the 32-pixel NESTED blocks b
-  // with b % nshards == shard (interleaved over the sky, so that the shards
-  // see the same mix of ray lengths); 0 of 1 for the whole shell
-  unsigned shard, nshards;
+  // shard `shard` of `nshards` of the shell: the NESTED blocks of
+  // 2^shard_log2 pixels b with b % nshards == shard (interleaved over the
+  // sky, so that the shards see the same mix of ray lengths; a block is a
+  // compact sky patch); 0 of 1 for the whole shell
+  unsigned shard, nshards, shard_log2;
   int do_dm, do_fd, do_sync;
   const double *fdmap;       // accumulated FD map of inner shells (or null)
   int nside_fdmap;
@@ -72,11 +73,12 @@ struct ShellLaunch {
 };
 
 // NESTED index of the shard's local pixel `local`: local pixels run through
-// the shard's 32-pixel blocks in order.
+// the shard's blocks in order.
 __device__ __forceinline__ unsigned long long shard_nest(const ShellLaunch &P,
                                                          unsigned long long local) {
   if (P.nshards == 1) return local;
-  return (((local >> 5) * P.nshards + P.shard) << 5) + (local & 31);
+  const unsigned L = P.shard_log2;
+  return (((local >> L) * P.nshards + P.shard) << L) + (local & ((1ull << L) - 1));
 }
 
 // Sample window [lo, hi) of one ray: the samples that can pass the

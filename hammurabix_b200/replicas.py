@@ -1,7 +1,7 @@
-"""Multi-process plumbing of the benchmark: one process per GPU, each an
-independent replica of the workload (the line-of-sight integration has no
-exchange step between replicas; pixel sharding would need the per-shell
-Faraday-depth map gathered before the next shell, integrator.cc:78-86).
+"""Multi-process plumbing of the benchmark: one process per GPU.  In
+replica mode each rank runs an independent copy of the workload (no
+exchange); the pixel-sharded pass (sharded.py) uses the same process group
+for its per-shell Faraday-depth all-reduce (integrator.cc:78-86).
 
 Timing follows the contract of the benchmark: every rank brackets its timed
 region with a barrier, the job time is the maximum over ranks, and the

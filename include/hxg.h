@@ -301,9 +301,10 @@ int hxg_sync(hxg_handle *h);
  * depth (integrator.cc:78-86).
  *
  * hxg_shell_integrate_device: radial integration of shell `shell` for the
- * pixels of shard `shard` of `nshards` (the 32-pixel NESTED blocks b with
- * b mod nshards == shard: interleaved over the sky, so every shard gets the
- * same mix of ray lengths) into the caller's shell maps at
+ * pixels of shard `shard` of `nshards` (NESTED blocks b of 2^k pixels with
+ * b mod nshards == shard, 32 <= 2^k <= 2048 and at least 8 blocks per shard
+ * where the shell allows: compact sky patches, interleaved so that every
+ * shard gets the same mix of ray lengths) into the caller's shell maps at
  * nside_shell[shell] (RING; d_tmp_fd is written whenever FD or sync is on).
  * With nshards > 1 the maps are zero outside the shard, so the shard maps of
  * all shards add up to the shell's maps.  d_fd = the accumulated FD output

@@ -25,11 +25,19 @@ from conftest import rel_err  # noqa: E402
 from hammurabix_b200 import abi, sharded, workloads as W  # noqa: E402
 
 
+def _block_log2(npix, n):
+    """The library's shard block size (shard_block_log2, hxg_api.cu)."""
+    L = 11
+    while L > 5 and (npix >> L) < 8 * n:
+        L -= 1
+    return L
+
+
 def _owned(npix, r, n):
-    """NESTED pixels of shard r of n: the 32-pixel blocks b with b % n == r
-    (the library's shard_nest, written out)."""
+    """NESTED pixels of shard r of n: the blocks b of 2^L pixels with
+    b % n == r (the library's shard_nest, written out)."""
     nest = np.arange(npix)
-    return (nest // 32) % n == r
+    return (nest >> _block_log2(npix, n)) % n == r
 
 
 class FakeIntegrator:
@@ -104,13 +112,14 @@ def test_two_gloo_ranks_reproduce_the_single_process_pass():
 def test_shards_partition_every_shell():
     """shard_nest (hxg_integrate.cuh) maps each shard's local pixels onto its
     blocks; over all shards every NESTED pixel is taken exactly once."""
-    for npix in (12, 48, 192, 768, 12 * 64 ** 2):
+    for npix in (12, 48, 192, 768, 12 * 64 ** 2, 12 * 256 ** 2):
         for n in (1, 2, 3, 8):
             seen = np.zeros(npix, dtype=int)
-            nblk = (npix + 31) // 32
+            L = _block_log2(npix, n)
+            nblk = (npix + (1 << L) - 1) >> L
             for r in range(n):
-                local = np.arange((nblk + n - 1 - r) // n * 32 if n > 1 else npix)
-                nest = local if n == 1 else ((local >> 5) * n + r) * 32 + (local & 31)
+                local = np.arange((nblk + n - 1 - r) // n << L if n > 1 else npix)
+                nest = local if n == 1 else (((local >> L) * n + r) << L) + (local & ((1 << L) - 1))
                 nest = nest[nest < npix]
                 assert np.all(_owned(npix, r, n)[nest])
                 seen[nest] += 1
