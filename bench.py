@@ -199,6 +199,43 @@ def run_reference_arm(args, wl):
     }), flush=True)
 
 
+def generators(args, dev, stream, torch):
+    """Device time of the random-field generators on the config-3 grid
+    geometry (512^3 over the 40 x 40 x 10 kpc box): Brnd_es with the
+    template's spectrum (rms 0.8 muG, k0 10, k1 0.1, a0 1.7, rho 3) along the
+    analytic spiral, and TErnd_dft (rms 0.01, k0 0.05, a0 -11/3).  Each call
+    is synchronous: k-space fill, cuFFT transforms (6 for Brnd_es, 1 for
+    TErnd_dft), the variance reduction and the real-space passes."""
+    import time as _t
+    from hammurabix_b200 import abi, workloads as W
+    from hammurabix_b200 import units as U
+    from hammurabix_b200.integrator import Integrator
+    n = WORKLOADS["config3"]["grid_n"]
+    desc = W.grid_desc(n)
+    obs = (-8.3 * U.kpc, 0.0, 0.006 * U.kpc)
+    es = abi.BrndEs(rms=0.8 * U.muGauss, k0=10.0, k1=0.1, a0=1.7, a1=0.0, rho=3.0,
+                    r0=8 * U.kpc, z0=1 * U.kpc)
+    dft = abi.TerndDft(rms=0.01, k0=0.05, a0=-11.0 / 3.0, r0=8 * U.kpc, z0=1 * U.kpc)
+    ig = Integrator("fp32c")
+    ig.set_stream(stream.cuda_stream)
+    ig.set_models(W.spiral_models())
+    res = {}
+    for name, fn in (("brnd_es", lambda k: ig.generate_brnd_es(desc, es, obs, 11 + k)),
+                     ("ternd_dft", lambda k: ig.generate_ternd_dft(desc, dft, obs, 21 + k))):
+        fn(0)                              # plans, workspace, first-touch
+        ts = []
+        for k in range(args.rfg_steps):
+            torch.cuda.synchronize(dev)
+            t0 = _t.perf_counter()
+            fn(k + 1)                      # synchronous on the handle's stream
+            ts.append(_t.perf_counter() - t0)
+        res[f"{name}_ms"] = 1e3 * sum(ts) / len(ts)
+    ig.close()
+    res["grid"] = f"{n}^3"
+    res["cells_per_s_brnd_es"] = n ** 3 / (res["brnd_es_ms"] / 1e3)
+    return res
+
+
 def adjoint_ratio(args, dev, stream, torch):
     """Adjoint vs forward device time on the config-4 workload: Nside
     64/128/256 over 3 shells to 30 kpc, 256^3 grids (B read as Grid_brnd,
@@ -336,6 +373,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=2)
     ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--rfg-steps", type=int, default=2)
     ap.add_argument("--mode", default="shard", choices=["shard", "replicas"],
                     help="N > 1: split each pass's shell pixels across the ranks with one FD "
                          "all-reduce per shell (shard, strong scaling) or run N independent "
@@ -535,6 +573,12 @@ def main():
         batch = batch_config5(args, dev, stream, torch)
         log(f"[rank {rank}] batch: {batch}")
 
+    # ---- random-field generators (Brnd_es, TErnd_dft) on the config-3 grid -------
+    rfg = None
+    if args.rfg_steps > 0:
+        rfg = generators(args, dev, stream, torch)
+        log(f"[rank {rank}] generators: {rfg}")
+
     # ---- roofline of the shell-integration kernel -------------------------------
     peak, peak_kind = measured_peaks()
     per_launch_s = kms / 1e3 / max(klaunch, 1)
@@ -585,6 +629,7 @@ def main():
             "adjoint_fwd_ratio": adjoint["ratio"] if adjoint else None,
             "adjoint": adjoint,
             "batch": batch,
+            "generators": rfg,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -87,6 +87,7 @@ struct hxg_handle {
   DevBuf grad_rec, grad_par, g_shell[5], g_fdmap;
   DevBuf ext;  // ExtModels block of the current launches
   DevBuf cre_tab;  // synchrotron tables + CRE energy tables
+  hxg::RfgWork *rfg = nullptr;  // random-field generator workspace
 };
 
 namespace {
@@ -882,10 +883,11 @@ int hxg_destroy(hxg_handle *h) {
     if (b.p) cudaFree(b.p);
   for (auto &b : h->ck_inner)
     if (b.p) cudaFree(b.p);
-  for (auto *b : {&h->grad_rec, &h->grad_par, &h->g_fdmap})
+  for (auto *b : {&h->grad_rec, &h->grad_par, &h->g_fdmap, &h->ext, &h->cre_tab})
     if (b->p) cudaFree(b->p);
   for (auto &b : h->g_shell)
     if (b.p) cudaFree(b.p);
+  rfg_release(h->rfg);
   for (auto &e : h->events) {
     cudaEventDestroy(e.first);
     cudaEventDestroy(e.second);
@@ -1138,7 +1140,7 @@ int hxg_generate_ternd_dft(hxg_handle *h, const hxg_grid_desc_t *g,
   int st = slot_prepare(h, HXG_FIELD_TERND, g, &n, &ncomp);
   if (st != HXG_OK) return st;
   Slot &S = h->slots[HXG_FIELD_TERND];
-  st = generate_ternd_dft(h->stream, *g, *p, observer, rfg_seed(seed), S.d[0]);
+  st = generate_ternd_dft(h->stream, h->rfg, *g, *p, observer, rfg_seed(seed), S.d[0]);
   h->launch_count += 4;  // fill, two reduction passes, rescale
   if (st != HXG_OK) return rfg_result(h, st, "ternd_dft");
   S.present = true;
@@ -1194,7 +1196,8 @@ int hxg_generate_brnd_es(hxg_handle *h, const hxg_grid_desc_t *g, const hxg_brnd
   int st = slot_prepare(h, HXG_FIELD_BRND, g, &n, &ncomp);
   if (st != HXG_OK) return st;
   Slot &S = h->slots[HXG_FIELD_BRND];
-  st = generate_brnd_es(h->stream, *g, *p, M, xb.p, bg, rfg_seed(seed), S.d[0], S.d[1], S.d[2]);
+  st = generate_brnd_es(h->stream, h->rfg, *g, *p, M, xb.p, bg, rfg_seed(seed), S.d[0], S.d[1],
+                        S.d[2]);
   h->launch_count += 7;  // fill, two reductions, rescale, project, repack, final
   if (st != HXG_OK) return rfg_result(h, st, "brnd_es");
   S.present = true;

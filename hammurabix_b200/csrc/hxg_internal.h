@@ -71,10 +71,16 @@ cudaError_t launch_unpack_grad(cudaStream_t s, uint64_t n, const double *rec,
                                double *gne);
 
 // Random-field generators (hxg_rfg.cu); synchronous on s, HXG_* status.
-int generate_ternd_dft(cudaStream_t s, const hxg_grid_desc_t &g, const hxg_ternd_dft_t &p,
-                       const double obs[3], uint64_t seed, double *te);
-int generate_brnd_es(cudaStream_t s, const hxg_grid_desc_t &g, const hxg_brnd_es_t &p,
-                     const DevModels &M, const ExtModels *ext, const RfgBregGrid &breg,
-                     uint64_t seed, double *bx, double *by, double *bz);
+// `work` is the caller's workspace (created on first use, kept for the next
+// call of the same grid shape, freed by rfg_release).
+struct RfgWork;
+void rfg_release(RfgWork *work);
+int generate_ternd_dft(cudaStream_t s, RfgWork *&work, const hxg_grid_desc_t &g,
+                       const hxg_ternd_dft_t &p, const double obs[3], uint64_t seed,
+                       double *te);
+int generate_brnd_es(cudaStream_t s, RfgWork *&work, const hxg_grid_desc_t &g,
+                     const hxg_brnd_es_t &p, const DevModels &M, const ExtModels *ext,
+                     const RfgBregGrid &breg, uint64_t seed, double *bx, double *by,
+                     double *bz);
 
 }  // namespace hxg

@@ -349,19 +349,28 @@ static RfgGrid rfg_grid(const hxg_grid_desc_t &g) {
   return G;
 }
 
-// RAII for the generator's device buffers and cuFFT plan
+// Workspace of the generators, kept on the handle between calls: the k-space
+// arrays, the reduction partials and the cuFFT plan of the last grid shape.
 struct RfgWork {
+  uint32_t nx = 0, ny = 0, nz = 0;
   double2 *c0 = nullptr, *c1 = nullptr;
   double *part = nullptr;
   cufftHandle plan = 0;
   bool have_plan = false;
-  ~RfgWork() {
+  void release() {
     if (have_plan) cufftDestroy(plan);
     if (c0) cudaFree(c0);
     if (c1) cudaFree(c1);
     if (part) cudaFree(part);
+    *this = RfgWork{};
   }
 };
+
+void rfg_release(RfgWork *w) {
+  if (!w) return;
+  w->release();
+  delete w;
+}
 
 static int rfg_status(cudaError_t e) {
   if (e == cudaSuccess) return HXG_OK;
@@ -384,22 +393,33 @@ static int fft_status(cufftResult r) {
     if (st_ != HXG_OK) return st_;                \
   } while (0)
 
-static int rfg_setup(cudaStream_t s, const hxg_grid_desc_t &g, bool two, RfgWork &W) {
+// Make the workspace fit grid g (two k-space arrays for Brnd_es); reuses
+// the previous buffers and plan when the shape is unchanged.
+static int rfg_setup(cudaStream_t s, const hxg_grid_desc_t &g, bool two, RfgWork *&pw) {
+  if (!pw) pw = new RfgWork;
+  RfgWork &W = *pw;
   const uint64_t n = (uint64_t)g.nx * g.ny * g.nz;
-  RFG_CK(cudaMalloc(&W.c0, n * sizeof(double2)));
-  if (two) RFG_CK(cudaMalloc(&W.c1, n * sizeof(double2)));
-  RFG_CK(cudaMalloc(&W.part, 1024 * sizeof(double)));
-  RFG_FFT(cufftPlan3d(&W.plan, (int)g.nx, (int)g.ny, (int)g.nz, CUFFT_Z2Z));
-  W.have_plan = true;
+  if (W.nx != g.nx || W.ny != g.ny || W.nz != g.nz) {
+    W.release();
+    RFG_CK(cudaMalloc(&W.c0, n * sizeof(double2)));
+    RFG_CK(cudaMalloc(&W.part, 1024 * sizeof(double)));
+    RFG_FFT(cufftPlan3d(&W.plan, (int)g.nx, (int)g.ny, (int)g.nz, CUFFT_Z2Z));
+    W.have_plan = true;
+    W.nx = g.nx;
+    W.ny = g.ny;
+    W.nz = g.nz;
+  }
+  if (two && !W.c1) RFG_CK(cudaMalloc(&W.c1, n * sizeof(double2)));
   RFG_FFT(cufftSetStream(W.plan, s));
   return HXG_OK;
 }
 
-int generate_ternd_dft(cudaStream_t s, const hxg_grid_desc_t &g, const hxg_ternd_dft_t &p,
-                       const double obs[3], uint64_t seed, double *te) {
-  RfgWork W;
-  int st = rfg_setup(s, g, false, W);
+int generate_ternd_dft(cudaStream_t s, RfgWork *&work, const hxg_grid_desc_t &g,
+                       const hxg_ternd_dft_t &p, const double obs[3], uint64_t seed,
+                       double *te) {
+  int st = rfg_setup(s, g, false, work);
   if (st != HXG_OK) return st;
+  RfgWork &W = *work;
   const RfgGrid G = rfg_grid(g);
   const uint64_t n = (uint64_t)g.nx * g.ny * g.nz;
   const hxg_brnd_es_t none{};
@@ -418,12 +438,13 @@ int generate_ternd_dft(cudaStream_t s, const hxg_grid_desc_t &g, const hxg_ternd
   return HXG_OK;
 }
 
-int generate_brnd_es(cudaStream_t s, const hxg_grid_desc_t &g, const hxg_brnd_es_t &p,
-                     const DevModels &M, const ExtModels *ext, const RfgBregGrid &breg,
-                     uint64_t seed, double *bx, double *by, double *bz) {
-  RfgWork W;
-  int st = rfg_setup(s, g, true, W);
+int generate_brnd_es(cudaStream_t s, RfgWork *&work, const hxg_grid_desc_t &g,
+                     const hxg_brnd_es_t &p, const DevModels &M, const ExtModels *ext,
+                     const RfgBregGrid &breg, uint64_t seed, double *bx, double *by,
+                     double *bz) {
+  int st = rfg_setup(s, g, true, work);
   if (st != HXG_OK) return st;
+  RfgWork &W = *work;
   const RfgGrid G = rfg_grid(g);
   const uint64_t n = (uint64_t)g.nx * g.ny * g.nz;
   const hxg_ternd_dft_t none{};

@@ -257,6 +257,9 @@ int hxg_export_grid_file(hxg_handle *h, int field, const char *path);
  * the Gaussian deviates of k-space cell c (x-major index, z fastest) are
  * Philox4x32-10 keyed by seed with counter {c, c >> 32, b, 0x52464721}
  * (b = 0, 1), through Box-Muller, so a field depends on the seed alone.
+ * The k-space workspace (16 bytes per cell, 32 for Brnd_es) and the FFT
+ * plan stay on the handle for the next call of the same grid shape;
+ * hxg_destroy releases them.
  * seed 0 draws a seed from the clock, as toolkit::random_seed(0) does
  * (include/toolkit.h:122-140).  observer = Param::observer (cm), used by
  * the spatial profile.  Synchronous.
