@@ -201,7 +201,8 @@ def run_reference_arm(args, wl):
 
 def generators(args, dev, stream, torch):
     """Device time of the random-field generators on the config-3 grid
-    geometry (512^3 over the 40 x 40 x 10 kpc box): Brnd_es with the
+    geometry (--rfg-grid cells per axis, 512 by default, over the
+    40 x 40 x 10 kpc box): Brnd_es with the
     template's spectrum (rms 0.8 muG, k0 10, k1 0.1, a0 1.7, rho 3) along the
     analytic spiral, and TErnd_dft (rms 0.01, k0 0.05, a0 -11/3).  Each call
     is synchronous: k-space fill, cuFFT transforms (6 for Brnd_es, 1 for
@@ -210,7 +211,7 @@ def generators(args, dev, stream, torch):
     from hammurabix_b200 import abi, workloads as W
     from hammurabix_b200 import units as U
     from hammurabix_b200.integrator import Integrator
-    n = WORKLOADS["config3"]["grid_n"]
+    n = args.rfg_grid
     desc = W.grid_desc(n)
     obs = (-8.3 * U.kpc, 0.0, 0.006 * U.kpc)
     es = abi.BrndEs(rms=0.8 * U.muGauss, k0=10.0, k1=0.1, a0=1.7, a1=0.0, rho=3.0,
@@ -374,6 +375,8 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=2)
     ap.add_argument("--batch-steps", type=int, default=2)
     ap.add_argument("--rfg-steps", type=int, default=2)
+    ap.add_argument("--rfg-grid", type=int, default=WORKLOADS["config3"]["grid_n"],
+                    help="cells per axis of the generator timing grid")
     ap.add_argument("--mode", default="shard", choices=["shard", "replicas"],
                     help="N > 1: split each pass's shell pixels across the ranks with one FD "
                          "all-reduce per shell (shard, strong scaling) or run N independent "
