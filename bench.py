@@ -413,8 +413,13 @@ def main():
     nout = max(wl["nside_shells"])
     npx = abi.npix(nout)
 
-    def outputs():
+    def maps5():
         return [torch.zeros(npx, dtype=torch.float64, device=dev) for _ in range(5)]
+
+    def outputs():
+        """One set of the five maps per pass: the fused passes write theirs
+        in the same traversal."""
+        return [maps5() for _ in passes]
 
     def make_integ(prec):
         ig = Integrator(prec, device=local)
@@ -424,41 +429,48 @@ def main():
         ig.upload_grid_device(abi.HXG_FIELD_TEREG, desc, f64[3:])
         return ig
 
+    def sel(o, m):
+        return [m[0] if o.do_dm else None, m[1] if o.do_fd else None, m[2], m[3], m[4]]
+
     # shard mode: shell maps for the per-shell exchange, summed with NCCL on
     # the launch stream (torch's current stream)
     shell_tmp = None
     if shard:
         import torch.distributed as dist
         nmax = max(abi.npix(n) for n in wl["nside_shells"])
-        shell_tmp = {k: torch.zeros(nmax, dtype=torch.float64, device=dev)
-                     for k in sharded.MAPS}
+        shell_tmp = sharded.make_shell_maps(
+            nmax, lambda n: torch.zeros(n, dtype=torch.float64, device=dev))
 
         def reduce_sum(t):
             dist.all_reduce(t)
 
-    def run_pass(ig, o, outs):
-        if shard:
-            sharded.write_grid_sharded(ig, o, dict(zip(sharded.MAPS, outs)), shell_tmp, rank,
-                                       ws, reduce_sum)
-        else:
-            ig.write_grid_device(o, outs[0] if o.do_dm else None, outs[1] if o.do_fd else None,
-                                 outs[2], outs[3], outs[4])
-
     def step(ig, outs):
-        for o in passes:
-            run_pass(ig, o, outs)
+        """One config-3 step: the frequency passes in the Pipeline's order,
+        fused into one traversal per shell where the form allows (FP32C)."""
+        if shard:
+            sharded.write_passes_sharded(ig, passes, [dict(zip(sharded.MAPS, m)) for m in outs],
+                                         shell_tmp, rank, ws, reduce_sum)
+        else:
+            ig.write_grid_multi_device([(o, sel(o, m)) for o, m in zip(passes, outs)])
+
+    def step_one_by_one(ig, outs):
+        """The passes one write_grid each, as the reference's Pipeline runs
+        them (the FP32C form's precision change alone)."""
+        for o, m in zip(passes, outs):
+            ig.write_grid_device(o, *sel(o, m))
 
     def barrier():
         torch.cuda.synchronize(dev)
         replicas.barrier(ws)
 
-    def timed(ig, outs, k):
+    def timed(ig, outs, k, fn=None):
+        fn = fn or step
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         barrier()
         ev0.record(stream)
         for _ in range(k):
-            step(ig, outs)
+            fn(ig, outs)
         ev1.record(stream)
         barrier()
         return ev0.elapsed_time(ev1) / 1e3
@@ -484,6 +496,16 @@ def main():
     ms_step = t32 / args.steps * 1e3
     log(f"[rank {rank}] fp32c: {ms_step:.1f} ms/step, {value:.4g} samples/s")
 
+    # ---- the same FP32C passes one by one (the precision change alone) ------
+    one_by_one = None
+    if not shard and args.fp64_steps > 0:
+        step_one_by_one(ig32, out32)
+        t1 = max_over_ranks(timed(ig32, out32, args.fp64_steps, step_one_by_one))
+        ms1 = t1 / args.fp64_steps * 1e3
+        one_by_one = {"ms_per_step": ms1, "ms_per_map": ms1 / len(passes),
+                      "samples_per_s": ws * samples_step / (ms1 / 1e3)}
+        log(f"[rank {rank}] fp32c passes one by one: {ms1:.1f} ms/step")
+
     # ---- plain FP64 GPU form on the same inputs ----------------------------
     fp64 = None
     errs = None
@@ -504,11 +526,8 @@ def main():
         errs = {}
         for idx in (0, len(passes) - 1):
             o = passes[idx]
-            a, b = outputs(), outputs()
-            ig32.write_grid_device(o, a[0] if o.do_dm else None, a[1] if o.do_fd else None,
-                                   a[2], a[3], a[4])
-            ig64.write_grid_device(o, b[0] if o.do_dm else None, b[1] if o.do_fd else None,
-                                   b[2], b[3], b[4])
+            a, b = out32[idx], maps5()      # the fused FP32C step's maps of this pass
+            ig64.write_grid_device(o, *sel(o, b))
             torch.cuda.synchronize(dev)
             tag = f"{o.sync_freq / 1e9:g}GHz"
             for j, k in enumerate(("dm", "fd", "I", "Q", "U")):
@@ -530,22 +549,22 @@ def main():
         pinned_out = [{k: torch.empty(npx, dtype=torch.float64, pin_memory=True).numpy()
                        for k in keys} for _ in passes]
         ige = Integrator("fp32c", device=local)
+        ige.set_stream(stream.cuda_stream)
         ige.set_models(models)
-        dev_out = outputs() if shard else None
+        dev_out = outputs()
 
         def e2e_step():
+            # grids from pinned host memory, the step on the device (the same
+            # fused or split passes as the product path), maps back to pinned
+            # host memory
             ige.upload_grid(abi.HXG_FIELD_BRND, desc, hosts[:3])
             ige.upload_grid(abi.HXG_FIELD_TEREG, desc, hosts[3:])
-            for o, po in zip(passes, pinned_out):
-                if shard:   # the split pass on device, then the maps to pinned host memory
-                    ige.set_stream(stream.cuda_stream)
-                    run_pass(ige, o, dev_out)
-                    for k, t in zip(keys, dev_out):
-                        if (k != "dm" or o.do_dm) and (k != "fd" or o.do_fd):
-                            torch.from_numpy(po[k]).copy_(t)
-                    torch.cuda.synchronize(dev)
-                else:
-                    ige.write_grid(o, out=po)
+            step(ige, dev_out)
+            for o, m, po in zip(passes, dev_out, pinned_out):
+                for k, t in zip(keys, sel(o, m)):
+                    if t is not None:
+                        torch.from_numpy(po[k]).copy_(t, non_blocking=True)
+            torch.cuda.synchronize(dev)
 
         e2e_step()
         barrier()
@@ -587,16 +606,22 @@ def main():
     per_launch_s = kms / 1e3 / max(klaunch, 1)
     samples_per_launch = ksamples / max(klaunch, 1)
     achieved = samples_per_launch * BYTES_PER_SAMPLE["fp32c"] / per_launch_s / 1e9
-    tps = traffic_per_sample("shell_fp32c_config3.md")
+    fused = len(passes) in (2, 3)
+    kname = (f"hxg::shell_fp32c_multi_kernel<1,false,{len(passes)}>" if fused
+             else "hxg::shell_fp32c_kernel<1,false>")
+    tps = traffic_per_sample("shell_fp32c_multi_config3.md" if fused
+                             else "shell_fp32c_config3.md")
     traffic = (tps * samples_per_launch) if tps else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                 "dram_gbs": traffic / per_launch_s / 1e9 if traffic else None,
                 "note": "achieved counts the 8-corner gather of the grid interpolation "
-                        f"({BYTES_PER_SAMPLE['fp32c']} B per sample); consecutive samples of a "
-                        "ray re-read the same voxels from L1/L2, so DRAM traffic stays far "
-                        "below it and the kernel is bound by instruction issue, not HBM",
-                "kernel": "hxg::shell_fp32c_kernel<1,false>",
+                        f"({BYTES_PER_SAMPLE['fp32c']} B per reference LOS sample); consecutive "
+                        "samples of a ray re-read the same voxels from L1/L2 and the fused "
+                        "kernel gathers once for the step's frequency passes, so DRAM traffic "
+                        "stays far below it and the kernel is bound by instruction issue, "
+                        "not HBM",
+                "kernel": kname,
                 "kernel_share_of_step": (kms / 1e3) / t32 if t32 > 0 else None,
                 "kernel_samples_per_s": ksamples / (kms / 1e3) if kms > 0 else None}
 
@@ -627,7 +652,13 @@ def main():
                                        f"replicas x{ws}" if ws > 1 else "1 GPU")},
             "ms_per_map": ms_step / len(passes),
             "fp64": fp64,
+            "fp32c_passes_one_by_one": one_by_one,
+            # the product step (passes fused into one traversal per shell)
+            # against the plain FP64 form, and the precision change alone
+            # (both forms pass by pass)
             "fp32c_speedup_vs_fp64": (fp64["ms_per_step"] / ms_step) if fp64 else None,
+            "fp32c_precision_speedup_vs_fp64": (fp64["ms_per_step"] / one_by_one["ms_per_step"]
+                                                if fp64 and one_by_one else None),
             "fp32c_max_rel_err_vs_fp64": errs,
             "adjoint_fwd_ratio": adjoint["ratio"] if adjoint else None,
             "adjoint": adjoint,

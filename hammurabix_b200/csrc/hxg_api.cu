@@ -69,6 +69,7 @@ struct hxg_handle {
   std::vector<double> mask_host;
   std::map<uint32_t, unsigned char *> mask_dev;
   DevBuf tmp[5];
+  DevBuf tmp_multi[6];  // I/Q/U shell maps of the 2nd and 3rd fused pass
   DevBuf out[5];
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -877,6 +878,8 @@ int hxg_destroy(hxg_handle *h) {
       if (p) cudaFree(p);
   for (auto &b : h->tmp)
     if (b.p) cudaFree(b.p);
+  for (auto &b : h->tmp_multi)
+    if (b.p) cudaFree(b.p);
   for (auto &b : h->out)
     if (b.p) cudaFree(b.p);
   for (auto &b : h->ck)
@@ -1391,6 +1394,188 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
   return HXG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Whether passes o[0..n) can share one shell traversal: FP32C form, the
+// same observer, shells, radial step, limits and mask switch, synchrotron on
+// in every pass, and no CRE grid (its emissivity depends on the frequency).
+bool fusable(const hxg_handle *h, const hxg_obs_t *o, int n) {
+  if (h->precision != HXG_FP32C || n < 2 || h->models.cre == HXG_CRE_GRID) return false;
+  for (int k = 0; k < n; ++k) {
+    const hxg_obs_t &a = o[0], &b = o[k];
+    if (!b.do_sync) return false;
+    if (std::memcmp(a.observer, b.observer, sizeof(a.observer)) != 0 ||
+        a.total_shell != b.total_shell || a.oc_r_res != b.oc_r_res ||
+        a.gc_r_min != b.gc_r_min || a.gc_r_max != b.gc_r_max || a.gc_z_min != b.gc_z_min ||
+        a.gc_z_max != b.gc_z_max || a.do_mask != b.do_mask)
+      return false;
+    for (uint32_t s = 0; s < a.total_shell; ++s)
+      if (a.nside_shell[s] != b.nside_shell[s]) return false;
+    for (uint32_t s = 0; s <= a.total_shell; ++s)
+      if (a.radii_shell[s] != b.radii_shell[s]) return false;
+  }
+  return true;
+}
+
+// One shell of NF fusable passes o[0..NF) over shard `shard` of `nshards`
+// into the shell maps tmp_dm, tmp_fd (shared) and tmp_iqu[f] (per pass);
+// fdmap = the accumulated FD output that passes with do_fd read.
+template <int NF>
+int fused_shell(hxg_handle *h, const hxg_obs_t *o, uint32_t s, uint32_t shard, uint32_t nshards,
+                const double *fdmap, int nside_fdmap, const ExtModels *ext_dev, double *tmp_dm,
+                double *tmp_fd, double *const (*tmp_iqu)[3]) {
+  const hxg_obs_t &o0 = o[0];
+  bool any_dm = false, any_fd = false;
+  for (int f = 0; f < NF; ++f) {
+    any_dm = any_dm || o[f].do_dm;
+    any_fd = any_fd || o[f].do_fd;
+  }
+  ShellLaunch P, Pf;
+  uint64_t step;
+  FreqSet<NF> Fq;
+  int st;
+  for (int f = NF - 1; f >= 0; --f) {  // P ends as pass 0's launch block
+    if ((st = build_launch(h, h->models, o[f], s, f == 0 ? P : Pf, step)) != HXG_OK) return st;
+    const ShellLaunch &L = f == 0 ? P : Pf;
+    Fq.lambda2[f] = L.lambda2;
+    Fq.phase_k[f] = L.phase_k;
+    Fq.k_t[f] = L.k_t;
+    Fq.k_p[f] = L.k_p;
+    Fq.tc_a[f] = L.tc_a;
+    Fq.tc_b[f] = L.tc_b;
+    Fq.a_s[f] = L.a_s;
+    Fq.inner[f] = o[f].do_fd ? 1 : 0;
+    for (int j = 0; j < 3; ++j) Fq.out[f][j] = tmp_iqu[f][j];
+  }
+  P.ext = ext_dev;
+  P.do_dm = any_dm;
+  P.do_fd = any_fd;
+  P.do_sync = 1;
+  P.fdmap = any_fd ? fdmap : nullptr;
+  P.nside_fdmap = any_fd ? nside_fdmap : 0;
+  P.mask = nullptr;
+  if (o0.do_mask) {
+    const unsigned char *dm = nullptr;
+    if ((st = device_mask(h, o0.nside_shell[s], &dm)) != HXG_OK) return st;
+    P.mask = dm;
+  }
+  P.out[0] = tmp_dm;
+  P.out[1] = tmp_fd;
+  P.out[2] = P.out[3] = P.out[4] = nullptr;
+  const uint64_t npix = npix_of(o0.nside_shell[s]);
+  P.shard = shard;
+  P.nshards = nshards;
+  P.shard_log2 = shard_block_log2(npix, nshards);
+  const uint64_t bsz = 1ull << P.shard_log2;
+  const uint64_t nblk = (npix + bsz - 1) / bsz;
+  const uint64_t local = nshards == 1 ? npix : (nblk + nshards - 1 - shard) / nshards * bsz;
+  const int C = choose_chunks(h, local, step);
+  P.chunks = C;
+  P.log2_chunks = hpx_ilog2((uint64_t)C);
+  if (local == 0) return HXG_OK;
+  const uint64_t warps = (local + (32 / C) - 1) / (32 / C);
+  const unsigned threads = 256;
+  const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (h->timing) {
+    HXG_CK(cudaEventCreate(&e0));
+    HXG_CK(cudaEventCreate(&e1));
+    HXG_CK(cudaEventRecord(e0, h->stream));
+  }
+  HXG_CK(launch_shell_multi(h->stream, P, NF, &Fq, blocks, threads));
+  ++h->launch_count;
+  if (h->timing) {
+    HXG_CK(cudaEventRecord(e1, h->stream));
+    h->events.emplace_back(e0, e1);
+    h->event_samples.push_back((int64_t)(std::min(local, npix) * step * NF));
+  }
+  return HXG_OK;
+}
+
+// nf (2 or 3) fusable passes in one traversal per shell; outs[5 k + j] =
+// map j (dm, fd, is, qs, us) of pass k.
+template <int NF>
+int write_fused(hxg_handle *h, const hxg_obs_t *o, double *const *outs) {
+  const hxg_obs_t &o0 = o[0];
+  uint32_t max_nside = 0;
+  for (uint32_t s = 0; s < o0.total_shell; ++s) max_nside = std::max(max_nside, o0.nside_shell[s]);
+  const size_t tbytes = npix_of(max_nside) * sizeof(double);
+  int st;
+  for (int k = 0; k < 5; ++k)
+    if ((st = ensure(h, h->tmp[k], tbytes)) != HXG_OK) return st;
+  for (int k = 0; k < 3 * (NF - 1); ++k)
+    if ((st = ensure(h, h->tmp_multi[k], tbytes)) != HXG_OK) return st;
+  double *tmp_dm = static_cast<double *>(h->tmp[0].p);
+  double *tmp_fd = static_cast<double *>(h->tmp[1].p);
+  double *tmp_iqu[NF][3];
+  for (int j = 0; j < 3; ++j) tmp_iqu[0][j] = static_cast<double *>(h->tmp[2 + j].p);
+  for (int f = 1; f < NF; ++f)
+    for (int j = 0; j < 3; ++j)
+      tmp_iqu[f][j] = static_cast<double *>(h->tmp_multi[3 * (f - 1) + j].p);
+  // the pass outputs start at zero (Grid_obs::build_grid, grid_obs.cc:21-43);
+  // the inner-shell FD is read from the first pass that accumulates FD
+  bool any_fd = false;
+  int fd_pass = -1;
+  for (int f = 0; f < NF; ++f) {
+    double *const *m = outs + 5 * f;
+    if (o[f].do_dm) HXG_CK(cudaMemsetAsync(m[0], 0, npix_of(o[f].nside_dm) * 8, h->stream));
+    if (o[f].do_fd) HXG_CK(cudaMemsetAsync(m[1], 0, npix_of(o[f].nside_fd) * 8, h->stream));
+    const size_t b = npix_of(o[f].nside_sync) * 8;
+    for (int j = 2; j < 5; ++j) HXG_CK(cudaMemsetAsync(m[j], 0, b, h->stream));
+    any_fd = any_fd || o[f].do_fd;
+    if (o[f].do_fd && fd_pass < 0) fd_pass = f;
+  }
+  const ExtModels *ext_dev = nullptr;
+  if ((st = upload_ext(h, h->models, o0.sync_freq, &ext_dev)) != HXG_OK) return st;
+  for (uint32_t s = 0; s < o0.total_shell; ++s) {
+    st = fused_shell<NF>(h, o, s, 0, 1, any_fd ? outs[5 * fd_pass + 1] : nullptr,
+                         any_fd ? (int)o[fd_pass].nside_fd : 0, ext_dev, tmp_dm, tmp_fd,
+                         tmp_iqu);
+    if (st != HXG_OK) return st;
+    // each pass merges the shared DM / FD maps it asks for and its own I/Q/U
+    for (int f = 0; f < NF; ++f) {
+      const double *t[5] = {tmp_dm, tmp_fd, tmp_iqu[f][0], tmp_iqu[f][1], tmp_iqu[f][2]};
+      double *const *m = outs + 5 * f;
+      if ((st = merge_shell(h, o[f], s, t, m[0], m[1], m[2], m[3], m[4])) != HXG_OK) return st;
+    }
+  }
+  h->ck_valid = false;
+  return HXG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hxg_write_grid_multi(hxg_handle *h, int npass, const hxg_obs_t *obs, double *const *d_outs) {
+  if (!h) return HXG_ERR_INVALID;
+  if (npass < 1 || !obs || !d_outs) return fail(h, HXG_ERR_INVALID, "bad pass list");
+  cudaSetDevice(h->device);
+  int st;
+  for (int k = 0; k < npass; ++k) {
+    double *const *m = d_outs + 5 * k;
+    if ((st = check_pass(h, obs + k, m[0], m[1], m[2] && m[3] && m[4])) != HXG_OK) return st;
+  }
+  int k = 0;
+  while (k < npass) {
+    const int left = npass - k;
+    const int nf = left >= 3 && fusable(h, obs + k, 3) ? 3 : (left >= 2 && fusable(h, obs + k, 2) ? 2 : 1);
+    if (nf == 3)
+      st = write_fused<3>(h, obs + k, d_outs + 5 * k);
+    else if (nf == 2)
+      st = write_fused<2>(h, obs + k, d_outs + 5 * k);
+    else {
+      double *const *m = d_outs + 5 * k;
+      st = hxg_write_grid_device(h, obs + k, m[0], m[1], m[2], m[3], m[4]);
+    }
+    if (st != HXG_OK) return st;
+    k += nf;
+  }
+  return HXG_OK;
+}
+
 int hxg_shell_integrate_device(hxg_handle *h, const hxg_obs_t *o, uint32_t shell,
                                uint32_t shard, uint32_t nshards, const double *d_fd,
                                double *d_tmp_dm, double *d_tmp_fd, double *d_tmp_is,
@@ -1414,6 +1599,52 @@ int hxg_shell_integrate_device(hxg_handle *h, const hxg_obs_t *o, uint32_t shell
   if ((st = upload_ext(h, h->models, o->sync_freq, &ext_dev)) != HXG_OK) return st;
   h->ck_valid = false;
   return run_shell(h, *o, shell, ext_dev, d_fd, tmp, shard, nshards, false);
+}
+
+int hxg_shell_integrate_multi_device(hxg_handle *h, int npass, const hxg_obs_t *o,
+                                     uint32_t shell, uint32_t shard, uint32_t nshards,
+                                     const double *d_fd, double *d_tmp_dm, double *d_tmp_fd,
+                                     double *const *d_tmp_iqu) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  if (!o || !d_tmp_iqu || npass < 2 || npass > 3 || shell >= o[0].total_shell ||
+      nshards == 0 || shard >= nshards)
+    return fail(h, HXG_ERR_INVALID, "bad pass count %d, shell %u or shard %u of %u", npass,
+                shell, shard, nshards);
+  int st;
+  bool any_fd = false;
+  int fd_pass = -1;
+  for (int f = 0; f < npass; ++f) {
+    const double *const *t = d_tmp_iqu + 3 * f;
+    if ((st = check_pass(h, o + f, d_tmp_dm, d_tmp_fd && (d_fd || !o[f].do_fd),
+                         t[0] && t[1] && t[2])) != HXG_OK)
+      return st;
+    any_fd = any_fd || o[f].do_fd;
+    if (o[f].do_fd && fd_pass < 0) fd_pass = f;
+  }
+  if (!d_tmp_fd) return fail(h, HXG_ERR_INVALID, "the shell FD map is always written");
+  if (!fusable(h, o, npass))
+    return fail(h, HXG_ERR_UNSUPPORTED, "these passes cannot share a traversal");
+  const uint64_t npix = npix_of(o[0].nside_shell[shell]);
+  double *tmp_iqu[3][3];
+  for (int f = 0; f < npass; ++f)
+    for (int j = 0; j < 3; ++j) tmp_iqu[f][j] = d_tmp_iqu[3 * f + j];
+  if (nshards > 1) {  // pixels of other shards stay zero: shard maps add up
+    std::vector<double *> all = {d_tmp_dm, d_tmp_fd};
+    for (int f = 0; f < npass; ++f)
+      for (int j = 0; j < 3; ++j) all.push_back(tmp_iqu[f][j]);
+    for (double *t : all)
+      if (t) HXG_CK(cudaMemsetAsync(t, 0, npix * sizeof(double), h->stream));
+  }
+  const ExtModels *ext_dev = nullptr;
+  if ((st = upload_ext(h, h->models, o[0].sync_freq, &ext_dev)) != HXG_OK) return st;
+  h->ck_valid = false;
+  const int nfd = any_fd ? (int)o[fd_pass].nside_fd : 0;
+  if (npass == 2)
+    return fused_shell<2>(h, o, shell, shard, nshards, d_fd, nfd, ext_dev, d_tmp_dm, d_tmp_fd,
+                          tmp_iqu);
+  return fused_shell<3>(h, o, shell, shard, nshards, d_fd, nfd, ext_dev, d_tmp_dm, d_tmp_fd,
+                        tmp_iqu);
 }
 
 int hxg_shell_merge_device(hxg_handle *h, const hxg_obs_t *o, uint32_t shell,

@@ -129,11 +129,48 @@ __device__ __forceinline__ double rsqrt_fd(double t) {
   return fma(0.5 * y, e, y);
 }
 
-// Warp gw of shell launch P (32/C pixels, C lanes each).  All 32 lanes of
-// the warp call it with the same gw.
-template <int NG, bool kExt>
-__device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw,
-                                           int lane) {
+template <int NF>
+__device__ __forceinline__ void combine_chunks_nf(const ShellLaunch &P, const FreqSet<NF> &Fq,
+                                                  int c, double &dm, double &fd, double si[NF],
+                                                  double sq[NF], double su[NF]) {
+  const int C = P.chunks;
+  if (C == 1) return;
+  // inclusive scan of fd within the segment
+  double incl = fd;
+  for (int o = 1; o < C; o <<= 1) {
+    const double v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (c >= o) incl += v;
+  }
+  double excl = __shfl_up_sync(0xffffffffu, incl, 1);
+  if (c == 0) excl = 0.;
+#pragma unroll
+  for (int f = 0; f < NF; ++f) {
+    if (P.do_sync && c > 0) {
+      double sr, cr;
+      sincos(2. * Fq.lambda2[f] * excl, &sr, &cr);
+      const double q = sq[f] * cr - su[f] * sr;
+      const double u = sq[f] * sr + su[f] * cr;
+      sq[f] = q;
+      su[f] = u;
+    }
+  }
+  for (int o = C >> 1; o > 0; o >>= 1) {
+    dm += shfl_xor_d(dm, o);
+    fd += shfl_xor_d(fd, o);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      si[f] += shfl_xor_d(si[f], o);
+      sq[f] += shfl_xor_d(sq[f], o);
+      su[f] += shfl_xor_d(su[f], o);
+    }
+  }
+}
+
+// Warp gw of shell launch P (32/C pixels, C lanes each) for the NF
+// frequency passes of Fq.  All 32 lanes of the warp call it with the same gw.
+template <int NG, bool kExt, int NF>
+__device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<NF> &Fq,
+                                           long long gw, int lane) {
   const int C = P.chunks;
   const int seg = lane >> P.log2_chunks;
   const int c = lane & (C - 1);
@@ -147,7 +184,9 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw,
     ring = hpx_nest2ring(h, nest);
     live = (P.mask == nullptr) || (P.mask[ring] != 0);
   }
-  double dm = 0., fd = 0., si = 0., sq = 0., su = 0.;
+  double dm = 0., fd = 0., si[NF], sq[NF], su[NF];
+#pragma unroll
+  for (int f = 0; f < NF; ++f) si[f] = sq[f] = su[f] = 0.;
   if (live) {
     double th, ph;
     hpx_pix2ang(h, ring, th, ph);
@@ -169,14 +208,19 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw,
     const double ou2 = 2. * (ox * ux + oy * uy + oz * uz);
     const double oo = ox * ox + oy * oy + oz * oz;
     const double r2min = P.gc_r_min * P.gc_r_min, r2max = P.gc_r_max * P.gc_r_max;
-    // Faraday phase in turns: rev0 + rev_k * (FD sum)
-    const double rev0 = P.lambda2 * inner * (1. / cgs::pi);
-    const double rev_k = P.phase_k * (0.5 / cgs::pi);
+    // Faraday phase in turns: rev0 + rev_k * (FD sum), per pass
+    double rev0[NF], rev_k[NF];
+    float a_s[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      rev0[f] = Fq.lambda2[f] * (Fq.inner[f] ? inner : 0.) * (1. / cgs::pi);
+      rev_k[f] = Fq.phase_k[f] * (0.5 / cgs::pi);
+      a_s[f] = float(Fq.a_s[f]);
+    }
     const DevModels &M = P.models;
     const FastModels &F = P.fast;
     const float pe = float(P.em_pe);
     const bool pe2 = P.em_const && P.em_pe == 2.;
-    const float a_s = float(P.a_s);
     const float cre_ir0 = float(1. / M.cre_r0), cre_2iz0 = float(2. / M.cre_z0);
     const float cre_R0 = float(M.cre_R0);
     // grid-space ray of group 0: g(d) = g0 + gv d
@@ -194,7 +238,13 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw,
     const double K0 = F.sp_sin * (ox * ux + oy * uy) + F.sp_cos * (ox * uy - oy * ux);
     const double K1 = F.sp_sin * (ux * ux + uy * uy);
     const float spf = float(F.sp_sin), cpf = float(F.sp_cos);
-    KahanF ki{0.f, 0.f}, kq{0.f, 0.f}, ku{0.f, 0.f};
+    // I is one sum for all passes when the emissivity weight is frequency
+    // independent (constant index); Q, U always one sum per pass
+    constexpr int NI = NF;
+    KahanF ki[NI], kq[NF], ku[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) ki[f] = kq[f] = ku[f] = KahanF{0.f, 0.f};
+    bool i_shared = true;
     double sfd = 0., sdm = 0.;
     const bool fast_b = M.breg == kBregSpiral;
     const bool slow_b = M.breg != kBregNone && M.breg != kBregGrid && !fast_b;
@@ -283,17 +333,22 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw,
         const float yv = -(etx * bx + ety * by + etz * bz);
         const float rr = fmaf(xv, xv, yv * yv);
         const float cc2 = fmaf(xv, xv, -yv * yv), ss2 = 2.f * xv * yv;
-        float wt, wpc, wps;
+        // emissivity weights: frequency independent (one set for all passes)
+        // except the variable-index form, whose A depends on the frequency
+        // through a_s; the host fuses no CRE-grid pass (its spectral
+        // integral depends on the frequency), so that branch reads pass 0
+        float wt[NF], wpc[NF], wps[NF];
+        bool shared_w = true;
         if (kExt && M.cre == kCreGrid) {
           // spectral integral over the CRE grid in FP64 (integrator.cc:288-330,
           // 357-400); scaled by 2^128 into FP32 range, k_t = k_p undo it
           double jt, jp;
           cre_grid_j(P.ext->cre, px, py, pz, double(sqrtf(rr)), jt, jp);
-          wt = float(jt * 0x1p128);
+          wt[0] = float(jt * 0x1p128);
           const float wp = float(jp * 0x1p128);
           const float inv = rr > 0.f ? __frcp_rn(rr) : 0.f;
-          wpc = rr > 0.f ? wp * cc2 * inv : wp;
-          wps = wp * ss2 * inv;
+          wpc[0] = rr > 0.f ? wp * cc2 * inv : wp;
+          wps[0] = wp * ss2 * inv;
         } else {
           float prof;
           if (M.cre == kCreAna) {
@@ -309,15 +364,16 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw,
             prof = cre_profile<float>(M, xf, yf, zf, p3);
           }
           if (pe2) {
-            wt = prof * rr;
-            wpc = prof * cc2;
-            wps = prof * ss2;
+            wt[0] = prof * rr;
+            wpc[0] = prof * cc2;
+            wps[0] = prof * ss2;
           } else {
-            float wp;
+            float wp[NF];
             if (P.em_const) {
               const float bp = (pe == 1.f) ? sqrtf(rr) : powf(rr, 0.5f * pe);
-              wt = wp = prof * bp;
+              wt[0] = wp[0] = prof * bp;
             } else {
+              shared_w = false;
               const float index = cre_index<float>(M, xf, yf, zf);
               if (index != last_index) {
                 gt = tgammaf(-0.25f * index + 19.f / 12.f) * tgammaf(-0.25f * index - 1.f / 12.f);
@@ -326,50 +382,99 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw,
                 last_index = index;
               }
               const float bper = sqrtf(rr);
-              const float Ae = exp2f(0.5f * (index + 1.f) * log2f(a_s / bper));
-              const float base = prof * bper * Ae;
-              wt = base * gt * inv1mi;
-              wp = base * gp;
+#pragma unroll
+              for (int f = 0; f < NF; ++f) {
+                const float Ae = exp2f(0.5f * (index + 1.f) * log2f(a_s[f] / bper));
+                const float base = prof * bper * Ae;
+                wt[f] = base * gt * inv1mi;
+                wp[f] = base * gp;
+              }
             }
             // ipa of a zero B_perp is 0 (atan2(0, 0)): cos 2ipa = 1
             const float inv = rr > 0.f ? __frcp_rn(rr) : 0.f;
-            wpc = rr > 0.f ? wp * cc2 * inv : wp;
-            wps = wp * ss2 * inv;
+#pragma unroll
+            for (int f = 0; f < (NF > 1 ? NF : 1); ++f) {
+              if (f > 0 && shared_w) break;
+              wpc[f] = rr > 0.f ? wp[f] * cc2 * inv : wp[f];
+              wps[f] = wp[f] * ss2 * inv;
+            }
           }
         }
-        ki.add(wt);
-        // Faraday phase: the turn count rev0 + rev_k * FD in FP64, its
-        // fraction rounded to 2^-23 turn in [-1/2, 1/2) with integer ops
-        const double rev = fma(rev_k, sfd, rev0) + 1572864.0;
-        const int q = (int)((unsigned)__double2loint(rev) + 256u) >> 9;
-        const float ang =
-            (__int_as_float(0x4B400000 + q) - 12582912.0f) * 7.490140565847857e-07f;
-        float sf, cf;
-        __sincosf(ang, &sf, &cf);
-        kq.add(fmaf(wpc, cf, -wps * sf));
-        ku.add(fmaf(wpc, sf, wps * cf));
+        if (shared_w) {
+#pragma unroll
+          for (int f = 1; f < NF; ++f) {
+            wt[f] = wt[0];
+            wpc[f] = wpc[0];
+            wps[f] = wps[0];
+          }
+          ki[0].add(wt[0]);
+        } else {
+#pragma unroll
+          for (int f = 0; f < NF; ++f) ki[f].add(wt[f]);
+        }
+        i_shared = shared_w;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+          // Faraday phase: the turn count rev0 + rev_k * FD in FP64, its
+          // fraction rounded to 2^-23 turn in [-1/2, 1/2) with integer ops
+          const double rev = fma(rev_k[f], sfd, rev0[f]) + 1572864.0;
+          const int q = (int)((unsigned)__double2loint(rev) + 256u) >> 9;
+          const float ang =
+              (__int_as_float(0x4B400000 + q) - 12582912.0f) * 7.490140565847857e-07f;
+          float sf, cf;
+          __sincosf(ang, &sf, &cf);
+          kq[f].add(fmaf(wpc[f], cf, -wps[f] * sf));
+          ku[f].add(fmaf(wpc[f], sf, wps[f] * cf));
+        }
       }
     }
     dm = sdm * P.k_dm;
     fd = sfd * P.fd_fore;
-    si = ki.value() * P.k_t;
-    sq = kq.value() * P.k_p;
-    su = ku.value() * P.k_p;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      si[f] = (i_shared ? ki[0] : ki[f]).value() * Fq.k_t[f];
+      sq[f] = kq[f].value() * Fq.k_p[f];
+      su[f] = ku[f].value() * Fq.k_p[f];
+    }
   }
-  combine_chunks(P, c, 2. * P.lambda2, dm, fd, si, sq, su);
+  combine_chunks_nf<NF>(P, Fq, c, dm, fd, si, sq, su);
   if (live && c == 0) {
     if (P.do_dm) P.out[0][ring] = dm;
     if (P.do_fd || P.do_sync) P.out[1][ring] = fd;
     if (P.do_sync) {
-      P.out[2][ring] = si * P.tc_a * P.tc_a / P.tc_b;
-      P.out[3][ring] = sq * P.tc_a * P.tc_a / P.tc_b;
-      P.out[4][ring] = su * P.tc_a * P.tc_a / P.tc_b;
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        Fq.out[f][0][ring] = si[f] * Fq.tc_a[f] * Fq.tc_a[f] / Fq.tc_b[f];
+        Fq.out[f][1][ring] = sq[f] * Fq.tc_a[f] * Fq.tc_a[f] / Fq.tc_b[f];
+        Fq.out[f][2][ring] = su[f] * Fq.tc_a[f] * Fq.tc_a[f] / Fq.tc_b[f];
+      }
     }
   } else if (valid && !live && c == 0) {
     if (P.do_dm) P.out[0][ring] = 0.;
     if (P.do_fd || P.do_sync) P.out[1][ring] = 0.;
-    if (P.do_sync) P.out[2][ring] = P.out[3][ring] = P.out[4][ring] = 0.;
+    if (P.do_sync) {
+#pragma unroll
+      for (int f = 0; f < NF; ++f) Fq.out[f][0][ring] = Fq.out[f][1][ring] = Fq.out[f][2][ring] = 0.;
+    }
   }
+}
+
+// One frequency pass: the pass's constants from its launch block.
+template <int NG, bool kExt>
+__device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw, int lane) {
+  FreqSet<1> Fq;
+  Fq.lambda2[0] = P.lambda2;
+  Fq.phase_k[0] = P.phase_k;
+  Fq.k_t[0] = P.k_t;
+  Fq.k_p[0] = P.k_p;
+  Fq.tc_a[0] = P.tc_a;
+  Fq.tc_b[0] = P.tc_b;
+  Fq.a_s[0] = P.a_s;
+  Fq.inner[0] = 1;
+  Fq.out[0][0] = P.out[2];
+  Fq.out[0][1] = P.out[3];
+  Fq.out[0][2] = P.out[4];
+  fp32c_tile<NG, kExt, 1>(P, Fq, gw, lane);
 }
 
 template <int NG, bool kExt>
@@ -377,6 +482,15 @@ __global__ void __launch_bounds__(256, HXG_FP32C_MIN_BLOCKS)
 shell_fp32c_kernel(const ShellLaunch P) {
   fp32c_tile<NG, kExt>(P, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
                        threadIdx.x & 31);
+}
+
+// NF frequency passes in one traversal of the shell (2 resident blocks: the
+// per-pass Q/U sums and phase constants take registers).
+template <int NG, bool kExt, int NF>
+__global__ void __launch_bounds__(256, 2)
+shell_fp32c_multi_kernel(const ShellLaunch P, const FreqSet<NF> Fq) {
+  fp32c_tile<NG, kExt, NF>(P, Fq, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                           threadIdx.x & 31);
 }
 
 }  // namespace hxg

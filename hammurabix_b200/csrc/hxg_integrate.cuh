@@ -72,6 +72,22 @@ struct ShellLaunch {
   const ExtModels *ext;  // Jaffe / JF12 / YMW16 blocks (device), or null
 };
 
+// The frequency-dependent constants of NF frequency passes that share one
+// shell traversal (same observer, shells, limits and models): each pass's
+// phase scale, emissivity scales, temp_convert and I/Q/U shell maps.  The
+// positions, field samples, emissivity weights, DM and FD of a sample do not
+// depend on the frequency and are computed once for all NF passes.
+template <int NF>
+struct FreqSet {
+  double lambda2[NF];   // (c/nu)^2
+  double phase_k[NF];   // 2 lambda^2 * fd_fore (per FP64 FD-sum unit)
+  double k_t[NF], k_p[NF];
+  double tc_a[NF], tc_b[NF];
+  double a_s[NF];       // A * |B_perp| scale of the variable-index emissivity
+  int inner[NF];        // 1: the pass reads the inner-shell FD (its do_fd)
+  double *out[NF][3];   // I, Q, U shell maps
+};
+
 // NESTED index of the shard's local pixel `local`: local pixels run through
 // the shard's blocks in order.
 __device__ __forceinline__ unsigned long long shard_nest(const ShellLaunch &P,

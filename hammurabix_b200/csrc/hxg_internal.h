@@ -48,6 +48,10 @@ cudaError_t launch_pack(cudaStream_t s, bool fp32, uint64_t n, void *rec,
                         double tscale);
 cudaError_t launch_shell(cudaStream_t s, bool fp32, const ShellLaunch &P,
                          unsigned blocks, unsigned threads);
+// nf = 2 or 3 frequency passes in one FP32C shell traversal; fq points to a
+// FreqSet<nf> (hxg_integrate.cuh).
+cudaError_t launch_shell_multi(cudaStream_t s, const ShellLaunch &P, int nf, const void *fq,
+                               unsigned blocks, unsigned threads);
 cudaError_t launch_accumulate_transpose(cudaStream_t s, int nside_out,
                                         int nside_shell, const double *g_out,
                                         double *g_shell, double scale);

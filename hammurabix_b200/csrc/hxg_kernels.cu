@@ -311,6 +311,20 @@ cudaError_t launch_shell(cudaStream_t s, bool fp32, const ShellLaunch &P,
   });
 }
 
+cudaError_t launch_shell_multi(cudaStream_t s, const ShellLaunch &P, int nf, const void *fq,
+                               unsigned blocks, unsigned threads) {
+  return by_shape(P.ngroups, P.ext != nullptr, [&](auto ng, auto ext) {
+    constexpr int NG = decltype(ng)::value;
+    constexpr bool E = decltype(ext)::value;
+    if (nf == 2)
+      shell_fp32c_multi_kernel<NG, E, 2>
+          <<<blocks, threads, 0, s>>>(P, *static_cast<const FreqSet<2> *>(fq));
+    else
+      shell_fp32c_multi_kernel<NG, E, 3>
+          <<<blocks, threads, 0, s>>>(P, *static_cast<const FreqSet<3> *>(fq));
+  });
+}
+
 cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups, bool ext,
                                const BatchLevel &B, unsigned blocks) {
   return by_shape(ngroups, ext, [&](auto ng, auto ex) {

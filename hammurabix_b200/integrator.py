@@ -137,6 +137,19 @@ class Integrator:
     def sync(self):
         _lib.check(self._lib.hxg_sync(self._h), self._h)
 
+    def write_grid_multi_device(self, passes):
+        """Several frequency passes at once (hxg_write_grid_multi): passes is
+        a list of (obs, [dm, fd, is, qs, us]) with torch CUDA float64 tensors
+        (None where the pass writes no such map).  In the FP32C form up to
+        three passes with the same geometry share one traversal per shell."""
+        n = len(passes)
+        obs = (abi.Obs * n)(*[o for o, _ in passes])
+        ptrs = (C.c_void_p * (5 * n))()
+        for k, (_, maps) in enumerate(passes):
+            for j, t in enumerate(maps):
+                ptrs[5 * k + j] = t.data_ptr() if t is not None else None
+        _lib.check(self._lib.hxg_write_grid_multi(self._h, n, obs, ptrs), self._h)
+
     # ---- one shell over a shard of its pixels ---------------------------------
     def shell_integrate_device(self, obs, shell, shard, nshards, fd, tmp):
         """Shell `shell` for the pixels of shard `shard` of `nshards` into the
@@ -147,6 +160,18 @@ class Integrator:
         _lib.check(self._lib.hxg_shell_integrate_device(
             self._h, C.byref(obs), int(shell), int(shard), int(nshards), ptr(fd),
             *(ptr(t) for t in tmp)), self._h)
+
+    def shell_integrate_multi_device(self, passes, shell, shard, nshards, fd, tmp_dm, tmp_fd,
+                                     tmp_iqu):
+        """hxg_shell_integrate_multi_device: 2 or 3 fusable passes (list of
+        Obs) in one traversal; tmp_iqu = one [I, Q, U] list per pass."""
+        n = len(passes)
+        obs = (abi.Obs * n)(*passes)
+        iqu = (C.c_void_p * (3 * n))(*[t.data_ptr() for maps in tmp_iqu for t in maps])
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        _lib.check(self._lib.hxg_shell_integrate_multi_device(
+            self._h, n, obs, int(shell), int(shard), int(nshards), ptr(fd), ptr(tmp_dm),
+            ptr(tmp_fd), iqu), self._h)
 
     def shell_merge_device(self, obs, shell, tmp, outs):
         """Accumulate shell maps tmp into the pass outputs outs = [dm, fd, is,

@@ -58,3 +58,72 @@ def write_grid_sharded(integ, obs, outs, tmp, rank, world, reduce_sum):
         for k in ("dm", "is", "qs", "us"):
             if req[k]:
                 reduce_sum(outs[k])
+
+
+def make_shell_maps(n, zeros):
+    """Shell-map buffers of n doubles for write_passes_sharded: the shared
+    DM and FD maps and I/Q/U for up to three fused passes; zeros(n) makes
+    one buffer."""
+    return {"dm": zeros(n), "fd": zeros(n),
+            "iqu": [[zeros(n) for _ in range(3)] for _ in range(3)]}
+
+
+def _fused_group(integ, group, outs, tmp, rank, world, reduce_sum):
+    """2 or 3 passes sharing one traversal per shell (the library refuses a
+    group it cannot fuse before any work, with HXG_ERR_UNSUPPORTED)."""
+    reqs = [requested(o) for o in group]
+    first = True
+    for s in range(group[0].total_shell):
+        n = abi.npix(group[0].nside_shell[s])
+        dm, fd = tmp["dm"][:n], tmp["fd"][:n]
+        iqu = [[t[:n] for t in tmp["iqu"][f]] for f in range(len(group))]
+        fd_out = next((outs[f]["fd"] for f, r in enumerate(reqs) if r["fd"]), None)
+        if first:
+            for f, r in enumerate(reqs):
+                for k in MAPS:
+                    if r[k]:
+                        outs[f][k].zero_()
+        integ.shell_integrate_multi_device(group, s, rank, world, fd_out, dm, fd, iqu)
+        first = False
+        if world > 1 and any(r["fd"] for r in reqs):
+            reduce_sum(fd)
+        for f, o in enumerate(group):
+            r = reqs[f]
+            integ.shell_merge_device(o, s, [dm if r["dm"] else None, fd] + iqu[f],
+                                     [outs[f][k] if r[k] else None for k in MAPS])
+    # every pass that writes FD merged the same complete maps: one FD output
+    # was read by the kernels, the others are copies of it
+    if world > 1:
+        for f, r in enumerate(reqs):
+            for k in ("dm", "is", "qs", "us"):
+                if r[k]:
+                    reduce_sum(outs[f][k])
+
+
+def write_passes_sharded(integ, passes, outs, tmp, rank, world, reduce_sum):
+    """Several frequency passes (the Pipeline's order) on this rank: groups
+    of up to three passes that the library can fuse share one traversal per
+    shell (hxg_shell_integrate_multi_device); the others run one by one.
+    outs: one dict of MAPS per pass; tmp: make_shell_maps(...)."""
+    from ._lib import HxgError
+    single = {"dm": tmp["dm"], "fd": tmp["fd"], "is": tmp["iqu"][0][0],
+              "qs": tmp["iqu"][0][1], "us": tmp["iqu"][0][2]}
+    k = 0
+    while k < len(passes):
+        done = False
+        for nf in (3, 2):
+            group = passes[k:k + nf]
+            if len(group) < nf:
+                continue
+            try:
+                _fused_group(integ, group, outs[k:k + nf], tmp, rank, world, reduce_sum)
+            except HxgError as e:
+                if e.status != abi.HXG_ERR_UNSUPPORTED:
+                    raise
+                continue
+            k += nf
+            done = True
+            break
+        if not done:
+            write_grid_sharded(integ, passes[k], outs[k], single, rank, world, reduce_sum)
+            k += 1

@@ -296,6 +296,23 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *obs, double *d_dm,
 /* Wait for the handle's stream; returns the first asynchronous error.     */
 int hxg_sync(hxg_handle *h);
 
+/* ---- several frequency passes at once -------------------------------------
+ * Pipeline::assemble_obs runs write_grid once per <sync> frequency
+ * (source/pipeline/pipeline.cc:165-190), each pass sampling the same rays
+ * at the same positions.  hxg_write_grid_multi takes the npass passes in
+ * that order (obs[k], outputs d_outs[5k .. 5k+4] = dm, fd, is, qs, us of
+ * pass k, as for hxg_write_grid_device) and, in the FP32C form, runs up to
+ * three consecutive passes that share observer, shells, radial step, limits
+ * and mask switch, all with synchrotron output and no CRE grid, in one
+ * traversal per shell: positions, field samples, emissivity weights, DM and
+ * FD once, then each pass's Faraday phase (with the inner-shell FD only for
+ * passes that request FD, as write_grid does) and I/Q/U sums.  Every map
+ * equals the one hxg_write_grid_device gives for that pass alone, to the
+ * FP32C tolerance.  Other passes run one by one.  Asynchronous on the
+ * handle's stream.  No counterpart in the reference.                       */
+int hxg_write_grid_multi(hxg_handle *h, int npass, const hxg_obs_t *obs,
+                         double *const *d_outs);
+
 /* ---- one shell at a time, over a shard of its pixels ---------------------
  * The two halves of one iteration of write_grid's shell loop
  * (integrator.cc:56-133), for callers that split a pass across GPUs: the
@@ -322,6 +339,15 @@ int hxg_shell_integrate_device(hxg_handle *h, const hxg_obs_t *obs, uint32_t she
                                uint32_t shard, uint32_t nshards, const double *d_fd,
                                double *d_tmp_dm, double *d_tmp_fd, double *d_tmp_is,
                                double *d_tmp_qs, double *d_tmp_us);
+/* The same for npass = 2 or 3 passes that hxg_write_grid_multi would fuse
+ * (else HXG_ERR_UNSUPPORTED): one traversal of the shard into the shared
+ * shell DM / FD maps and the per-pass I, Q, U shell maps d_tmp_iqu[3k ..
+ * 3k+2]; each pass then merges with hxg_shell_merge_device (the DM / FD
+ * shell maps are the same for every pass that requests them).            */
+int hxg_shell_integrate_multi_device(hxg_handle *h, int npass, const hxg_obs_t *obs,
+                                     uint32_t shell, uint32_t shard, uint32_t nshards,
+                                     const double *d_fd, double *d_tmp_dm, double *d_tmp_fd,
+                                     double *const *d_tmp_iqu);
 int hxg_shell_merge_device(hxg_handle *h, const hxg_obs_t *obs, uint32_t shell,
                            const double *d_tmp_dm, const double *d_tmp_fd,
                            const double *d_tmp_is, const double *d_tmp_qs,

@@ -54,6 +54,19 @@ class FakeIntegrator:
             t.zero_()
             t[own] = (k + 1) * base[own] + 1e-3 * inner
 
+    def shell_integrate_multi_device(self, passes, s, shard, nshards, fd, dm_t, fd_t, iqu):
+        n = abi.npix(passes[0].nside_shell[s])
+        own = torch.from_numpy(_owned(n, shard, nshards))
+        inner = float(fd.sum()) if fd is not None else 0.0
+        base = 1.0 + s + 0.01 * torch.arange(n, dtype=torch.float64)
+        for k, t in enumerate([dm_t, fd_t]):
+            t.zero_()
+            t[own] = (k + 1) * base[own]
+        for f, o in enumerate(passes):
+            for j, t in enumerate(iqu[f]):
+                t.zero_()
+                t[own] = (3 + j) * base[own] * (1 + 0.1 * f) + 1e-3 * inner * o.do_fd
+
     def shell_merge_device(self, obs, s, tmp, outs):
         for t, o in zip(tmp, outs):
             if t is None or o is None:
@@ -75,6 +88,20 @@ def _run(world, rank, reduce_sum):
     return {k: v.numpy().copy() for k, v in outs.items()}
 
 
+def _passes():
+    return W.frequency_passes(W.make_obs([4, 8, 8], 20.0, 0.1, freq_ghz=1.4), [0.408, 1.4, 30.0])
+
+
+def _run_passes(world, rank, reduce_sum):
+    ps = _passes()
+    out_n = abi.npix(8)
+    z = lambda n: torch.zeros(n, dtype=torch.float64)
+    outs = [{k: z(out_n) for k in sharded.MAPS} for _ in ps]
+    sharded.write_passes_sharded(FakeIntegrator(), ps, outs, sharded.make_shell_maps(out_n, z),
+                                 rank, world, reduce_sum)
+    return [{k: v.numpy().copy() for k, v in o.items()} for o in outs]
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -87,12 +114,16 @@ def _rank(rank, ws, port, q):
     import torch.distributed as dist
     from hammurabix_b200 import replicas
     w, r, _ = replicas.init("gloo", 60)
-    q.put((r, _run(w, r, lambda t: dist.all_reduce(t))))
+    red = lambda t: dist.all_reduce(t)
+    q.put((r, (_run(w, r, red), _run_passes(w, r, red))))
     replicas.finish(w)
 
 
 def test_two_gloo_ranks_reproduce_the_single_process_pass():
+    """One pass (per-shell exchange) and three fused passes of the
+    Pipeline's order, on two ranks, against one process."""
     single = _run(1, 0, None)
+    single_multi = _run_passes(1, 0, None)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
@@ -104,9 +135,15 @@ def test_two_gloo_ranks_reproduce_the_single_process_pass():
         p.join(timeout=60)
         assert p.exitcode == 0
     for r in (0, 1):
+        one, multi = got[r]
         for k in sharded.MAPS:
             assert np.abs(single[k]).max() > 0, k
-            assert rel_err(got[r][k], single[k]) <= 1e-12, (r, k)
+            assert rel_err(one[k], single[k]) <= 1e-12, (r, k)
+        for p, (a, b) in enumerate(zip(multi, single_multi)):
+            for k in sharded.MAPS:
+                if sharded.requested(_passes()[p])[k]:
+                    assert np.abs(b[k]).max() > 0, (p, k)
+                    assert rel_err(a[k], b[k]) <= 1e-12, (r, p, k)
 
 
 def test_shards_partition_every_shell():
@@ -187,3 +224,61 @@ def test_emulated_shards_match_the_unsplit_pass(fields32, precision, tol, nshard
                 a, b = got[j].cpu().numpy(), ref[j].cpu().numpy()
                 assert rel_err(a, b) <= tol, (k, rel_err(a, b))
                 assert np.abs(b).max() > 0, k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nshards", [1, 3])
+def test_emulated_shards_of_fused_passes(fields32, nshards):
+    """Three fused passes (hxg_shell_integrate_multi_device) split into
+    shards run one after another, against the passes one by one."""
+    from hammurabix_b200.integrator import Integrator
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    bx, by, bz, ne = (torch.tensor(np.asarray(a, dtype=np.float64).reshape(-1), device=dev)
+                      for a in fields32)
+    passes = W.frequency_passes(W.make_obs([8, 16, 32], 20.0, 0.05, freq_ghz=0.408),
+                                [0.408, 1.4, 30.0])
+    z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev) if n else None
+    with Integrator("fp32c") as integ:
+        integ.set_stream(stream.cuda_stream)
+        integ.set_models(W.grid_models())
+        integ.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(32), [bx, by, bz])
+        integ.upload_grid_device(abi.HXG_FIELD_TEREG, W.grid_desc(32), [ne])
+        ref = []
+        for o in passes:
+            ndm, nfd, nsy = abi.obs_output_sizes(o)
+            m = [z(ndm), z(nfd), z(nsy), z(nsy), z(nsy)]
+            integ.write_grid_device(o, *m)
+            ref.append(m)
+        reqs = [sharded.requested(o) for o in passes]
+        outs = [[[z(n) for n in abi.obs_output_sizes(o)[:2]] + [z(abi.obs_output_sizes(o)[2])
+                                                                for _ in range(3)]
+                 for o in passes] for _ in range(nshards)]
+        fd = outs[0][0][1]                       # pass 0's FD output, shared by the shards
+        for s in range(passes[0].total_shell):
+            n = abi.npix(passes[0].nside_shell[s])
+            parts = []
+            for r in range(nshards):
+                t = {"dm": z(n), "fd": z(n), "iqu": [[z(n) for _ in range(3)] for _ in passes]}
+                integ.shell_integrate_multi_device(passes, s, r, nshards, fd, t["dm"], t["fd"],
+                                                   t["iqu"])
+                parts.append(t)
+            fd_sum = sum(t["fd"] for t in parts)             # the per-shell all-reduce
+            for r in range(nshards):
+                for f, o in enumerate(passes):
+                    rq = reqs[f]
+                    tmp = [parts[r]["dm"] if rq["dm"] else None, fd_sum] + parts[r]["iqu"][f]
+                    out = list(outs[r][f])
+                    if rq["fd"]:
+                        out[1] = fd if r == 0 else z(len(fd))   # one FD output for all
+                    integ.shell_merge_device(o, s, tmp, [out[j] if rq[k] else None
+                                                         for j, k in enumerate(sharded.MAPS)])
+        integ.sync()
+        for f, o in enumerate(passes):
+            for j, k in enumerate(sharded.MAPS):
+                if not reqs[f][k]:
+                    continue
+                got = fd if k == "fd" else sum(outs[r][f][j] for r in range(nshards))
+                e = rel_err(got.cpu().numpy(), ref[f][j].cpu().numpy())
+                assert e <= 1e-5, (f, k, e)
