@@ -137,6 +137,25 @@ class Integrator:
     def sync(self):
         _lib.check(self._lib.hxg_sync(self._h), self._h)
 
+    def write_grid_multi(self, passes):
+        """Host-side hxg_write_grid_multi: passes is a list of Obs; returns
+        one dict dm/fd/is/qs/us of float64 numpy maps per pass (None where
+        the pass writes no such map).  The device maps are torch tensors
+        written on the handle's stream; the call waits for it."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        keys = ("dm", "fd", "is", "qs", "us")
+        dev_maps = []
+        for o in passes:
+            ndm, nfd, nsy = abi.obs_output_sizes(o)
+            dev_maps.append([torch.empty(n, dtype=torch.float64, device=dev) if n else None
+                             for n in (ndm, nfd, nsy, nsy, nsy)])
+        torch.cuda.synchronize(dev)           # allocations settled before the library writes
+        self.write_grid_multi_device(list(zip(passes, dev_maps)))
+        self.sync()
+        return [{k: (t.cpu().numpy() if t is not None else None) for k, t in zip(keys, maps)}
+                for maps in dev_maps]
+
     def write_grid_multi_device(self, passes):
         """Several frequency passes at once (hxg_write_grid_multi): passes is
         a list of (obs, [dm, fd, is, qs, us]) with torch CUDA float64 tensors

@@ -71,9 +71,11 @@ class Pipeline:
             self.assemble_fields()
         self.maps = {}
         self.raw = []
-        for k in range(par.num_passes()):
-            o = par.obs_pass(k)
-            out = self.integ.write_grid(o)
+        # all passes in one call: the FP32C form runs passes of the same
+        # geometry in one traversal per shell (hxg_write_grid_multi)
+        obs = [par.obs_pass(k) for k in range(par.num_passes())]
+        outs = self.integ.write_grid_multi(obs)
+        for k, (o, out) in enumerate(zip(obs, outs)):
             self.raw.append((o, out))
             idx = len(par.do_sync) - 1 - k
             if o.do_dm:
