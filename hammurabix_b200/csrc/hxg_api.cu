@@ -1326,22 +1326,26 @@ int run_shell(hxg_handle *h, const hxg_obs_t &o, uint32_t s, const ExtModels *ex
 int merge_shell(hxg_handle *h, const hxg_obs_t &o, uint32_t s, const double *const tmp[5],
                 double *d_dm, double *d_fd, double *d_is, double *d_qs, double *d_us) {
   const int ns = (int)o.nside_shell[s];
-  if (o.do_dm) {
-    double *d[1] = {d_dm};
-    const double *sr[1] = {tmp[0]};
-    HXG_CK(launch_accumulate(h->stream, (int)o.nside_dm, ns, 1, d, sr));
-    ++h->launch_count;
-  }
-  if (o.do_sync) {
-    double *d[3] = {d_is, d_qs, d_us};
-    const double *sr[3] = {tmp[2], tmp[3], tmp[4]};
-    HXG_CK(launch_accumulate(h->stream, (int)o.nside_sync, ns, 3, d, sr));
-    ++h->launch_count;
-  }
-  if (o.do_fd) {
-    double *d[1] = {d_fd};
-    const double *sr[1] = {tmp[1]};
-    HXG_CK(launch_accumulate(h->stream, (int)o.nside_fd, ns, 1, d, sr));
+  // one merge launch per output Nside (DM, FD and I/Q/U usually share one)
+  const bool want[5] = {o.do_dm != 0, o.do_fd != 0, o.do_sync != 0, o.do_sync != 0,
+                        o.do_sync != 0};
+  const uint32_t nside[5] = {o.nside_dm, o.nside_fd, o.nside_sync, o.nside_sync,
+                             o.nside_sync};
+  double *const out[5] = {d_dm, d_fd, d_is, d_qs, d_us};
+  bool done[5] = {false, false, false, false, false};
+  for (int a = 0; a < 5; ++a) {
+    if (!want[a] || done[a]) continue;
+    double *d[5];
+    const double *sr[5];
+    int n = 0;
+    for (int b = a; b < 5; ++b)
+      if (want[b] && !done[b] && nside[b] == nside[a]) {
+        d[n] = out[b];
+        sr[n] = tmp[b];
+        ++n;
+        done[b] = true;
+      }
+    HXG_CK(launch_accumulate(h->stream, (int)nside[a], ns, n, d, sr));
     ++h->launch_count;
   }
   return HXG_OK;
@@ -1534,11 +1538,29 @@ int write_fused(hxg_handle *h, const hxg_obs_t *o, double *const *outs) {
                          any_fd ? (int)o[fd_pass].nside_fd : 0, ext_dev, tmp_dm, tmp_fd,
                          tmp_iqu);
     if (st != HXG_OK) return st;
-    // each pass merges the shared DM / FD maps it asks for and its own I/Q/U
+    // each pass merges the shared DM / FD maps it asks for and its own
+    // I/Q/U: one merge launch per output Nside for all passes' maps
+    std::vector<std::pair<uint32_t, std::pair<double *, const double *>>> pairs;
     for (int f = 0; f < NF; ++f) {
-      const double *t[5] = {tmp_dm, tmp_fd, tmp_iqu[f][0], tmp_iqu[f][1], tmp_iqu[f][2]};
       double *const *m = outs + 5 * f;
-      if ((st = merge_shell(h, o[f], s, t, m[0], m[1], m[2], m[3], m[4])) != HXG_OK) return st;
+      if (o[f].do_dm) pairs.push_back({o[f].nside_dm, {m[0], tmp_dm}});
+      if (o[f].do_fd) pairs.push_back({o[f].nside_fd, {m[1], tmp_fd}});
+      for (int j = 0; j < 3; ++j) pairs.push_back({o[f].nside_sync, {m[2 + j], tmp_iqu[f][j]}});
+    }
+    std::vector<bool> done(pairs.size(), false);
+    for (size_t a = 0; a < pairs.size(); ++a) {
+      if (done[a]) continue;
+      std::vector<double *> d;
+      std::vector<const double *> sr;
+      for (size_t b = a; b < pairs.size(); ++b)
+        if (!done[b] && pairs[b].first == pairs[a].first) {
+          d.push_back(pairs[b].second.first);
+          sr.push_back(pairs[b].second.second);
+          done[b] = true;
+        }
+      HXG_CK(launch_accumulate(h->stream, (int)pairs[a].first, (int)o0.nside_shell[s],
+                               (int)d.size(), d.data(), sr.data()));
+      ++h->launch_count;
     }
   }
   h->ck_valid = false;

@@ -13,19 +13,22 @@
 namespace hxg {
 
 // ---- Hampix::accumulate (include/hamdis.h:698-721) ----------------------
-// dst_k += src_k for up to 3 map pairs sharing one (nside_dst, nside_src);
-// when the Nsides differ, src is interpolated at each dst pixel's pointing.
-__global__ void accumulate_kernel(int nside_dst, int nside_src, int nmaps,
-                                  double *d0, const double *s0, double *d1,
-                                  const double *s1, double *d2,
-                                  const double *s2) {
+// dst_k += src_k for up to kMaxMergeMaps map pairs sharing one (nside_dst,
+// nside_src); when the Nsides differ, src is interpolated at each dst
+// pixel's pointing (the pointing and the 4 weights once for all maps).
+constexpr int kMaxMergeMaps = 12;
+struct MergeMaps {
+  int n;
+  double *dst[kMaxMergeMaps];
+  const double *src[kMaxMergeMaps];
+};
+
+__global__ void accumulate_kernel(int nside_dst, int nside_src, MergeMaps M) {
   const Hpx hd = hpx_make((uint64_t)nside_dst);
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= hd.npix) return;
-  double *dst[3] = {d0, d1, d2};
-  const double *src[3] = {s0, s1, s2};
   if (nside_dst == nside_src) {
-    for (int k = 0; k < nmaps; ++k) dst[k][i] = dst[k][i] + src[k][i];
+    for (int k = 0; k < M.n; ++k) M.dst[k][i] = M.dst[k][i] + M.src[k][i];
     return;
   }
   const Hpx hs = hpx_make((uint64_t)nside_src);
@@ -34,8 +37,8 @@ __global__ void accumulate_kernel(int nside_dst, int nside_src, int nmaps,
   uint64_t pix[4];
   double w[4];
   hpx_interp_weights(hs, th, ph, pix, w);
-  for (int k = 0; k < nmaps; ++k)
-    dst[k][i] = dst[k][i] + hpx_interp_apply(src[k], pix, w);
+  for (int k = 0; k < M.n; ++k)
+    M.dst[k][i] = M.dst[k][i] + hpx_interp_apply(M.src[k], pix, w);
 }
 
 __global__ void pix2ang_kernel(int nside, uint64_t n, double *theta,
@@ -225,11 +228,18 @@ cudaError_t launch_accumulate(cudaStream_t s, int nside_dst, int nside_src,
                               int nmaps, double *const *dst,
                               const double *const *src) {
   const uint64_t n = 12ull * nside_dst * nside_dst;
-  accumulate_kernel<<<blocks_for(n, 256), 256, 0, s>>>(
-      nside_dst, nside_src, nmaps, dst[0], src[0], nmaps > 1 ? dst[1] : nullptr,
-      nmaps > 1 ? src[1] : nullptr, nmaps > 2 ? dst[2] : nullptr,
-      nmaps > 2 ? src[2] : nullptr);
-  return cudaGetLastError();
+  for (int k0 = 0; k0 < nmaps; k0 += kMaxMergeMaps) {
+    MergeMaps M{};
+    M.n = nmaps - k0 < kMaxMergeMaps ? nmaps - k0 : kMaxMergeMaps;
+    for (int k = 0; k < M.n; ++k) {
+      M.dst[k] = dst[k0 + k];
+      M.src[k] = src[k0 + k];
+    }
+    accumulate_kernel<<<blocks_for(n, 256), 256, 0, s>>>(nside_dst, nside_src, M);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_pix2ang(cudaStream_t s, int nside, uint64_t n,
