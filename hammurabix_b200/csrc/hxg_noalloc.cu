@@ -1,10 +1,9 @@
 // hxg_noalloc.cu -- the allocation-free variant of the FP64 integrator.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
-// being captured (an allocation would end the capture), plugins that live
-// inside a host application which owns every device allocation through its
-// own pool, and real-time pipelines that must not touch the allocator after
-// start-up.  hxg_write_grid_noalloc serves them: it takes device inputs and
+// Some callers cannot call cudaMalloc: plugins that live inside a host
+// application which owns every device allocation through its own pool, and
+// real-time pipelines whose memory is fixed at start-up and which must not
+// touch the allocator afterwards.  hxg_write_grid_noalloc serves them: it takes device inputs and
 // device outputs from the caller and keeps its only scratch -- the five
 // per-shell HEALPix maps -- in the fixed-size array below.
 //

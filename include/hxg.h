@@ -437,10 +437,11 @@ int hxg_get_launch_count(hxg_handle *h, int64_t *count);
 
 /* ---- allocation-free integration ---------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate
- * device memory -- code running during CUDA graph capture, plugins whose
- * host application owns every device allocation, pipelines that must not
- * touch the allocator after start-up -- this entry point runs the FP64
- * integrator without any cudaMalloc/cudaFree.  Inputs and outputs are the
+ * device memory -- plugins whose host application owns every device
+ * allocation through its own pool, pipelines whose memory is fixed at
+ * start-up and must not touch the allocator afterwards -- this entry
+ * point runs the FP64 integrator without any cudaMalloc/cudaFree.  Inputs
+ * and outputs are the
  * caller's device buffers; the only scratch (the per-shell HEALPix maps) is
  * a fixed static device array of 5 x 12 x HXG_NOALLOC_MAX_NSIDE^2 doubles
  * (7.5 MiB) that every GPU loading the library holds until exit.

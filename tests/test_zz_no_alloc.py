@@ -1,6 +1,6 @@
 """hxg_write_grid_noalloc: the integrator for callers that cannot allocate
-device memory (graph capture, host applications that own every device
-allocation, allocator-free real-time loops).  It must give the same maps as
+device memory (host applications that own every device allocation,
+real-time loops that must not touch the allocator after start-up).  It must give the same maps as
 the ordinary entry point, twice in a row, with its scratch held in a fixed
 static device array.  Collected last so that a failure here leaves the rest
 of the suite already run."""
