@@ -442,8 +442,9 @@ int hxg_get_launch_count(hxg_handle *h, int64_t *count);
  * start-up and must not touch the allocator afterwards -- this entry
  * point runs the FP64 integrator without any cudaMalloc/cudaFree.  Inputs
  * and outputs are the caller's device buffers; the only scratch (the
- * per-shell HEALPix maps) is a fixed static device array of 5 x 12 x HXG_NOALLOC_MAX_NSIDE^2 doubles
- * (7.5 MiB) that every GPU loading the library holds until exit.
+ * per-shell HEALPix maps) is a fixed static device array of
+ * 5 x 12 x HXG_NOALLOC_MAX_NSIDE^2 doubles (7.5 MiB) that every GPU loading
+ * the library holds until exit.
  *
  *  - grid / d_records: one packed grid of FP64 voxel records
  *    {bx, by, bz, ne} (32 B per voxel, x-major, z fastest), holding the sum
