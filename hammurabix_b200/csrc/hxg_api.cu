@@ -1405,8 +1405,9 @@ namespace {
 // Whether passes o[0..n) can share one shell traversal: FP32C form, the
 // same observer, shells, radial step, limits and mask switch, synchrotron on
 // in every pass, and no CRE grid (its emissivity depends on the frequency).
-bool fusable(const hxg_handle *h, const hxg_obs_t *o, int n) {
-  if (h->precision != HXG_FP32C || n < 2 || h->models.cre == HXG_CRE_GRID) return false;
+// Passes o[0..n) with synchrotron output and the same observer, shells,
+// radial step, limits and mask switch: one traversal can serve them all.
+bool same_traversal(const hxg_obs_t *o, int n) {
   for (int k = 0; k < n; ++k) {
     const hxg_obs_t &a = o[0], &b = o[k];
     if (!b.do_sync) return false;
@@ -1421,6 +1422,13 @@ bool fusable(const hxg_handle *h, const hxg_obs_t *o, int n) {
       if (a.radii_shell[s] != b.radii_shell[s]) return false;
   }
   return true;
+}
+
+// Whether passes o[0..n) of the handle's models can share one traversal:
+// FP32C form, no CRE grid (its emissivity depends on the frequency).
+bool fusable(const hxg_handle *h, const hxg_obs_t *o, int n) {
+  if (h->precision != HXG_FP32C || n < 2 || h->models.cre == HXG_CRE_GRID) return false;
+  return same_traversal(o, n);
 }
 
 // One shell of NF fusable passes o[0..NF) over shard `shard` of `nshards`
@@ -2094,12 +2102,16 @@ struct hxg_batch {
   DevBuf tmp, zeros, zblocks, counters;
   DevBuf ext;               // ExtModels per entry (entries that use them)
   bool ext_any = false;
+  // plan tables per (level, class): class c holds plans of c + 1 fused
+  // frequency passes, at index 3 * level + c
   std::vector<DevBuf> plans, tiles, merges, mblocks;
   std::vector<int> nplans, nmerge;
   std::vector<unsigned long long> merge_blocks;
+  std::vector<int> group;  // passes fused with entry i (0: inside a group)
   int nzero = 0;
   unsigned long long zero_blocks = 0;
-  unsigned level_blocks = 0;
+  unsigned level_blocks[3] = {0, 0, 0};
+  int graph_kernels = 0;  // kernels one run of the graph launches
   cudaGraphExec_t exec = nullptr;
 };
 
@@ -2137,52 +2149,130 @@ int batch_tables(hxg_batch *b, int lanes, int grain) {
   b->grain = grain;
   b->samples = 0;
   double *tmp = static_cast<double *>(b->tmp.p);
+  const auto map = [&](size_t i, int k) { return tmp + b->tmp_off[i] + k * b->tmp_n[i]; };
   for (int s = 0; s < b->levels; ++s) {
-    std::vector<ShellLaunch> P;
-    std::vector<unsigned long long> t0(1, 0ull);
+    std::vector<ShellLaunch> P1;
+    std::vector<hxg::FusedPlan<2>> P2;
+    std::vector<hxg::FusedPlan<3>> P3;
+    std::vector<unsigned long long> t0[3];
+    for (auto &t : t0) t.assign(1, 0ull);
     std::vector<MergeJob> mj;
     std::vector<unsigned long long> m0(1, 0ull);
-    for (size_t i = 0; i < b->e.size(); ++i) {
+    const auto job = [&](int nmaps, double *const *d, const double *const *src, uint32_t nd,
+                         int ns) {
+      MergeJob J{};
+      for (int q = 0; q < nmaps; ++q) {
+        J.dst[q] = d[q];
+        J.src[q] = src[q];
+      }
+      J.nmaps = nmaps;
+      J.nside_dst = (int)nd;
+      J.nside_src = ns;
+      mj.push_back(J);
+      m0.push_back(m0.back() + (npix_of(nd) + 255) / 256);
+    };
+    for (size_t i = 0; i < b->e.size(); i += (size_t)b->group[i]) {
+      const int nf = b->group[i];
       const hxg_batch_entry_t &E = b->e[i];
       const hxg_obs_t &o = E.obs;
       if ((uint32_t)s >= o.total_shell) continue;
       ShellLaunch L;
       uint64_t step;
       if ((st = build_launch(h, E.models, o, (uint32_t)s, L, step)) != HXG_OK) return st;
-      L.fdmap = o.do_fd ? E.d_fd : nullptr;
-      L.nside_fdmap = o.do_fd ? (int)o.nside_fd : 0;
       L.mask = nullptr;
       L.ext = uses_ext(E.models) ? static_cast<const ExtModels *>(b->ext.p) + i : nullptr;
-      double *t = tmp + b->tmp_off[i];
-      for (int k = 0; k < 5; ++k) L.out[k] = t + k * b->tmp_n[i];
       int C = std::min(lanes, 32);
       while (C > 1 && step / (uint64_t)C < 16) C >>= 1;
       L.chunks = C;
       L.log2_chunks = hxg::hpx_ilog2((uint64_t)C);
       const uint64_t npix = npix_of(o.nside_shell[s]);
-      P.push_back(L);
-      t0.push_back(t0.back() + (npix * C + 31) / 32);
-      b->samples += (int64_t)(npix * step);
       const int ns = (int)o.nside_shell[s];
-      const auto job = [&](int nmaps, double *d0, double *d1, double *d2, int kk, uint32_t nd) {
-        MergeJob J{};
-        J.dst[0] = d0; J.dst[1] = d1; J.dst[2] = d2;
-        for (int q = 0; q < nmaps; ++q) J.src[q] = t + (kk + q) * b->tmp_n[i];
-        J.nmaps = nmaps;
-        J.nside_dst = (int)nd;
-        J.nside_src = ns;
-        mj.push_back(J);
-        m0.push_back(m0.back() + (npix_of(nd) + 255) / 256);
+      const unsigned long long tiles = (npix * C + 31) / 32;
+      b->samples += (int64_t)(npix * step * nf);
+      // inner-shell FD and the shared DM / FD shell maps: the first pass of
+      // the group that accumulates FD; DM / FD shell maps live in the
+      // group's first entry
+      size_t fd_entry = i;
+      bool any_dm = false, any_fd = false;
+      for (int f = nf - 1; f >= 0; --f) {
+        any_dm = any_dm || b->e[i + f].obs.do_dm;
+        if (b->e[i + f].obs.do_fd) {
+          any_fd = true;
+          fd_entry = i + f;
+        }
+      }
+      L.fdmap = any_fd ? b->e[fd_entry].d_fd : nullptr;
+      L.nside_fdmap = any_fd ? (int)b->e[fd_entry].obs.nside_fd : 0;
+      for (int k = 0; k < 5; ++k) L.out[k] = map(i, k);
+      if (nf > 1) {
+        L.do_dm = any_dm;
+        L.do_fd = any_fd;
+        L.do_sync = 1;
+        L.out[2] = L.out[3] = L.out[4] = nullptr;
+      }
+      const auto freqs = [&](auto &F) -> int {
+        for (int f = 0; f < nf; ++f) {
+          ShellLaunch Lf;
+          uint64_t sf;
+          const int r = build_launch(h, b->e[i + f].models, b->e[i + f].obs, (uint32_t)s, Lf, sf);
+          if (r != HXG_OK) return r;
+          F.lambda2[f] = Lf.lambda2;
+          F.phase_k[f] = Lf.phase_k;
+          F.k_t[f] = Lf.k_t;
+          F.k_p[f] = Lf.k_p;
+          F.tc_a[f] = Lf.tc_a;
+          F.tc_b[f] = Lf.tc_b;
+          F.a_s[f] = Lf.a_s;
+          F.inner[f] = b->e[i + f].obs.do_fd ? 1 : 0;
+          for (int j = 0; j < 3; ++j) F.out[f][j] = map(i + f, 2 + j);
+        }
+        return HXG_OK;
       };
-      if (o.do_dm) job(1, E.d_dm, nullptr, nullptr, 0, o.nside_dm);
-      if (o.do_sync) job(3, E.d_is, E.d_qs, E.d_us, 2, o.nside_sync);
-      if (o.do_fd) job(1, E.d_fd, nullptr, nullptr, 1, o.nside_fd);
+      if (nf == 1) {
+        P1.push_back(L);
+      } else if (nf == 2) {
+        hxg::FusedPlan<2> FP;
+        FP.P = L;
+        if ((st = freqs(FP.F)) != HXG_OK) return st;
+        P2.push_back(FP);
+      } else {
+        hxg::FusedPlan<3> FP;
+        FP.P = L;
+        if ((st = freqs(FP.F)) != HXG_OK) return st;
+        P3.push_back(FP);
+      }
+      t0[nf - 1].push_back(t0[nf - 1].back() + tiles);
+      for (int f = 0; f < nf; ++f) {
+        const hxg_batch_entry_t &Ef = b->e[i + f];
+        const hxg_obs_t &of = Ef.obs;
+        if (of.do_dm) {
+          double *d[1] = {Ef.d_dm};
+          const double *sr[1] = {map(i, 0)};
+          job(1, d, sr, of.nside_dm, ns);
+        }
+        if (of.do_sync) {
+          double *d[3] = {Ef.d_is, Ef.d_qs, Ef.d_us};
+          const double *sr[3] = {map(i + f, 2), map(i + f, 3), map(i + f, 4)};
+          job(3, d, sr, of.nside_sync, ns);
+        }
+        if (of.do_fd) {
+          double *d[1] = {Ef.d_fd};
+          const double *sr[1] = {map(i, 1)};
+          job(1, d, sr, of.nside_fd, ns);
+        }
+      }
     }
-    b->nplans[s] = (int)P.size();
+    const int c0 = 3 * s;
+    b->nplans[c0] = (int)P1.size();
+    b->nplans[c0 + 1] = (int)P2.size();
+    b->nplans[c0 + 2] = (int)P3.size();
     b->nmerge[s] = (int)mj.size();
     b->merge_blocks[s] = m0.back();
-    if ((st = upload_vec(h, b->plans[s], P)) != HXG_OK) return st;
-    if ((st = upload_vec(h, b->tiles[s], t0)) != HXG_OK) return st;
+    if ((st = upload_vec(h, b->plans[c0], P1)) != HXG_OK) return st;
+    if ((st = upload_vec(h, b->plans[c0 + 1], P2)) != HXG_OK) return st;
+    if ((st = upload_vec(h, b->plans[c0 + 2], P3)) != HXG_OK) return st;
+    for (int c = 0; c < 3; ++c)
+      if ((st = upload_vec(h, b->tiles[c0 + c], t0[c])) != HXG_OK) return st;
     if ((st = upload_vec(h, b->merges[s], mj)) != HXG_OK) return st;
     if ((st = upload_vec(h, b->mblocks[s], m0)) != HXG_OK) return st;
   }
@@ -2203,17 +2293,33 @@ int batch_capture(hxg_batch *b) {
                                          static_cast<const unsigned long long *>(b->zblocks.p),
                                          b->nzero, b->zero_blocks);
   unsigned long long *ctr = static_cast<unsigned long long *>(b->counters.p);
+  b->graph_kernels = 1 + b->levels;  // zeroing, one merge per level
   for (int l = 0; l < b->levels && e == cudaSuccess; ++l) {
-    e = cudaMemsetAsync(ctr + l, 0, sizeof(unsigned long long), s);
-    if (e != cudaSuccess) break;
-    BatchLevel B;
-    B.plans = static_cast<const ShellLaunch *>(b->plans[l].p);
-    B.tile_start = static_cast<const unsigned long long *>(b->tiles[l].p);
-    B.nplans = b->nplans[l];
-    B.grain = b->grain;
-    B.counter = ctr + l;
-    if (B.nplans > 0)
-      e = hxg::launch_batch_level(s, b->fp32, b->ngroups, b->ext_any, B, b->level_blocks);
+    for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
+      const int k = 3 * l + c;
+      if (b->nplans[k] == 0) continue;
+      ++b->graph_kernels;
+      e = cudaMemsetAsync(ctr + k, 0, sizeof(unsigned long long), s);
+      if (e != cudaSuccess) break;
+      const auto *tiles = static_cast<const unsigned long long *>(b->tiles[k].p);
+      if (c == 0) {
+        BatchLevel B;
+        B.plans = static_cast<const ShellLaunch *>(b->plans[k].p);
+        B.tile_start = tiles;
+        B.nplans = b->nplans[k];
+        B.grain = b->grain;
+        B.counter = ctr + k;
+        e = hxg::launch_batch_level(s, b->fp32, b->ngroups, b->ext_any, B, b->level_blocks[0]);
+      } else if (c == 1) {
+        hxg::BatchLevelMulti<2> B{static_cast<const hxg::FusedPlan<2> *>(b->plans[k].p), tiles,
+                                  b->nplans[k], b->grain, ctr + k};
+        e = hxg::launch_batch_level_multi(s, b->ngroups, b->ext_any, 2, &B, b->level_blocks[1]);
+      } else {
+        hxg::BatchLevelMulti<3> B{static_cast<const hxg::FusedPlan<3> *>(b->plans[k].p), tiles,
+                                  b->nplans[k], b->grain, ctr + k};
+        e = hxg::launch_batch_level_multi(s, b->ngroups, b->ext_any, 3, &B, b->level_blocks[2]);
+      }
+    }
     if (e != cudaSuccess) break;
     e = hxg::launch_batch_merge(s, static_cast<const MergeJob *>(b->merges[l].p),
                                 static_cast<const unsigned long long *>(b->mblocks[l].p),
@@ -2321,11 +2427,11 @@ int hxg_batch_create(hxg_handle *h, int n, const hxg_batch_entry_t *entries,
   }
   b->nzero = (int)zj.size();
   b->zero_blocks = z0.back();
-  b->plans.resize(b->levels);
-  b->tiles.resize(b->levels);
+  b->plans.resize(3 * b->levels);
+  b->tiles.resize(3 * b->levels);
   b->merges.resize(b->levels);
   b->mblocks.resize(b->levels);
-  b->nplans.assign(b->levels, 0);
+  b->nplans.assign(3 * b->levels, 0);
   b->nmerge.assign(b->levels, 0);
   b->merge_blocks.assign(b->levels, 0ull);
   const auto bail = [&](int code) {
@@ -2334,8 +2440,28 @@ int hxg_batch_create(hxg_handle *h, int n, const hxg_batch_entry_t *entries,
     return code;
   };
   if ((st = ensure(h, b->tmp, total * sizeof(double))) != HXG_OK) return bail(st);
-  if ((st = ensure(h, b->counters, b->levels * sizeof(unsigned long long))) != HXG_OK)
+  if ((st = ensure(h, b->counters, 3 * b->levels * sizeof(unsigned long long))) != HXG_OK)
     return bail(st);
+  // frequency passes of one parameter set that can share a traversal: up to
+  // three consecutive entries with the same models and geometry (FP32C form,
+  // synchrotron in every pass, no CRE grid)
+  b->group.assign(b->e.size(), 0);
+  for (size_t i = 0; i < b->e.size();) {
+    int nf = 1;
+    for (int cand = 3; b->fp32 && cand >= 2 && nf == 1; --cand) {
+      if (i + cand > b->e.size() || b->e[i].models.cre == HXG_CRE_GRID) continue;
+      hxg_obs_t o[3];
+      bool same = true;
+      for (int f = 0; f < cand; ++f) {
+        o[f] = b->e[i + f].obs;
+        same = same && std::memcmp(&b->e[i].models, &b->e[i + f].models,
+                                   sizeof(hxg_models_t)) == 0;
+      }
+      if (same && same_traversal(o, cand)) nf = cand;
+    }
+    b->group[i] = nf;
+    i += nf;
+  }
   if ((st = upload_vec(h, b->zeros, zj)) != HXG_OK) return bail(st);
   if ((st = upload_vec(h, b->zblocks, z0)) != HXG_OK) return bail(st);
   {
@@ -2355,7 +2481,12 @@ int hxg_batch_create(hxg_handle *h, int n, const hxg_batch_entry_t *entries,
   int per_sm = 0;
   cudaError_t ce = hxg::batch_level_occupancy(b->fp32, b->ngroups, b->ext_any, &per_sm);
   if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "occupancy"));
-  b->level_blocks = (unsigned)std::max(1, per_sm) * (unsigned)h->sm_count;
+  b->level_blocks[0] = (unsigned)std::max(1, per_sm) * (unsigned)h->sm_count;
+  for (int nf = 2; nf <= 3 && b->fp32; ++nf) {
+    ce = hxg::batch_multi_occupancy(b->ngroups, b->ext_any, nf, &per_sm);
+    if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "occupancy"));
+    b->level_blocks[nf - 1] = (unsigned)std::max(1, per_sm) * (unsigned)h->sm_count;
+  }
   // launch shapes: lanes per pixel x tiles per work fetch
   const int shapes[][2] = {{1, 4}, {2, 4}, {4, 4}, {8, 4}, {1, 16}, {2, 1}};
   int best = 0;
@@ -2385,7 +2516,7 @@ int hxg_batch_run(hxg_batch *b) {
   hxg_handle *h = b->h;
   cudaSetDevice(h->device);
   HXG_CK(cudaGraphLaunch(b->exec, h->stream));
-  h->launch_count += 1 + 2 * b->levels;
+  h->launch_count += b->graph_kernels;
   return HXG_OK;
 }
 

@@ -23,6 +23,60 @@ struct BatchLevel {
   unsigned long long *counter;
 };
 
+// A plan of NF frequency passes of one parameter set fused into one
+// traversal (the FP32C form; fp32c_tile<NG, kExt, NF>).
+template <int NF>
+struct FusedPlan {
+  ShellLaunch P;
+  FreqSet<NF> F;
+};
+
+// The same work distribution over fused plans.
+template <int NF>
+struct BatchLevelMulti {
+  const FusedPlan<NF> *plans;
+  const unsigned long long *tile_start;
+  int nplans;
+  int grain;
+  unsigned long long *counter;
+};
+
+// Plan index of tile t0: the last plan whose first tile is <= t0.
+__device__ __forceinline__ int batch_plan_of(const unsigned long long *tile_start, int nplans,
+                                             unsigned long long t0) {
+  int lo = 0, hi = nplans - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_start[mid] <= t0) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int NG, bool kExt, int NF>
+__device__ __forceinline__ void batch_multi_body(const BatchLevelMulti<NF> &B) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long total = B.tile_start[B.nplans];
+  for (;;) {
+    unsigned long long t0 = 0;
+    if (lane == 0) t0 = atomicAdd(B.counter, (unsigned long long)B.grain);
+    t0 = __shfl_sync(0xffffffffu, t0, 0);
+    if (t0 >= total) return;
+    const unsigned long long t1 = min(t0 + (unsigned long long)B.grain, total);
+    int k = batch_plan_of(B.tile_start, B.nplans, t0);
+    for (unsigned long long t = t0; t < t1; ++t) {
+      while (t >= B.tile_start[k + 1]) ++k;
+      const FusedPlan<NF> &FP = B.plans[k];
+      fp32c_tile<NG, kExt, NF>(FP.P, FP.F, (long long)(t - B.tile_start[k]), lane);
+    }
+  }
+}
+
+template <int NG, bool kExt, int NF>
+__global__ void __launch_bounds__(256, 2)
+batch_fp32c_multi_kernel(const BatchLevelMulti<NF> B) {
+  batch_multi_body<NG, kExt, NF>(B);
+}
+
 template <int NG, bool kFp32, bool kExt>
 __device__ __forceinline__ void batch_level_body(const BatchLevel &B) {
   const int lane = threadIdx.x & 31;

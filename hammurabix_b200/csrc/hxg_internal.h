@@ -60,6 +60,10 @@ cudaError_t launch_adjoint(cudaStream_t s, const AdjointLaunch &A,
 cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups, bool ext,
                                const BatchLevel &B, unsigned blocks);
 cudaError_t batch_level_occupancy(bool fp32, int ngroups, bool ext, int *blocks_per_sm);
+// Fused-frequency plans (nf = 2 or 3): B points to a BatchLevelMulti<nf>.
+cudaError_t launch_batch_level_multi(cudaStream_t s, int ngroups, bool ext, int nf,
+                                     const void *B, unsigned blocks);
+cudaError_t batch_multi_occupancy(int ngroups, bool ext, int nf, int *blocks_per_sm);
 cudaError_t launch_batch_merge(cudaStream_t s, const MergeJob *jobs,
                                const unsigned long long *block0, int njobs,
                                unsigned long long nblocks);

@@ -345,6 +345,33 @@ cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups, bool ext,
   });
 }
 
+cudaError_t launch_batch_level_multi(cudaStream_t s, int ngroups, bool ext, int nf,
+                                     const void *B, unsigned blocks) {
+  return by_shape(ngroups, ext, [&](auto ng, auto ex) {
+    constexpr int NG = decltype(ng)::value;
+    constexpr bool E = decltype(ex)::value;
+    if (nf == 2)
+      batch_fp32c_multi_kernel<NG, E, 2>
+          <<<blocks, 256, 0, s>>>(*static_cast<const BatchLevelMulti<2> *>(B));
+    else
+      batch_fp32c_multi_kernel<NG, E, 3>
+          <<<blocks, 256, 0, s>>>(*static_cast<const BatchLevelMulti<3> *>(B));
+  });
+}
+
+cudaError_t batch_multi_occupancy(int ngroups, bool ext, int nf, int *blocks_per_sm) {
+  const void *f = nullptr;
+  by_shape(ngroups, ext, [&](auto ng, auto ex) {
+    constexpr int NG = decltype(ng)::value;
+    constexpr bool E = decltype(ex)::value;
+    if (nf == 2)
+      f = (const void *)batch_fp32c_multi_kernel<NG, E, 2>;
+    else
+      f = (const void *)batch_fp32c_multi_kernel<NG, E, 3>;
+  });
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, 256, 0);
+}
+
 cudaError_t batch_level_occupancy(bool fp32, int ngroups, bool ext, int *blocks_per_sm) {
   const void *f = nullptr;
   by_shape(ngroups, ext, [&](auto ng, auto ex) {

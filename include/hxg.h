@@ -404,6 +404,10 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *obs,
  *    that merges the shell maps into the outputs; an entry's outer shells
  *    read the Faraday depth its inner shells accumulated, as in
  *    write_grid;
+ *  - in the FP32C form, up to three consecutive entries with the same
+ *    models and geometry and synchrotron output (one parameter set at
+ *    several frequencies, as hxg_write_grid_multi takes them; no CRE grid)
+ *    share one traversal per shell;
  *  - tune != 0: the launch shapes (lanes per pixel x tiles per fetch) are
  *    timed once in hxg_batch_create and the fastest is kept;
  *  - hxg_batch_run launches the graph on the handle's stream and does not

@@ -93,3 +93,48 @@ def test_batch_rejects_mismatched_grid_reads_and_masks(fields32):
         with pytest.raises(_lib.HxgError) as e:
             integ.batch([(m, masked, _outs(o, dev))])
         assert e.value.status == abi.HXG_ERR_UNSUPPORTED
+
+
+def test_batch_fuses_the_frequencies_of_a_parameter_set(fields32):
+    """Consecutive entries with the same models and geometry (one parameter
+    set at several frequencies, the first with DM and FD) share one
+    traversal per shell in the FP32C batch; every entry's maps equal the
+    pass run alone.  A lone entry and a pair sit between the groups."""
+    dev = torch.device("cuda", 0)
+    rng = np.random.Generator(np.random.PCG64(11))
+    bx, by, bz, ne = (torch.tensor(np.asarray(a, dtype=np.float64).reshape(-1), device=dev)
+                      for a in fields32)
+    ents = []
+    for nf in (3, 1, 2, 3):
+        m = W.grid_models(W.spiral_models(b0_muG=rng.uniform(2, 8),
+                                          pitch_deg=rng.uniform(-40, -5)))
+        nsides = [8 * 2 ** s for s in range(int(rng.integers(1, 4)))]
+        rmax = rng.uniform(15, 30)
+        for k, f in enumerate((30.0, 1.4, 0.408)[:nf]):
+            ents.append((m, W.make_obs(nsides, rmax, 0.05, freq_ghz=f, do_dm=(k == 0),
+                                       do_fd=(k == 0))))
+    with I.Integrator("fp32c") as integ:
+        integ.set_models(ents[0][0])
+        integ.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(32), [bx, by, bz])
+        integ.upload_grid_device(abi.HXG_FIELD_TEREG, W.grid_desc(32), [ne])
+        ref = []
+        for m, o in ents:
+            integ.set_models(m)
+            outs = _outs(o, dev)
+            integ.write_grid_device(o, outs["dm"], outs["fd"], outs["is"], outs["qs"], outs["us"])
+            ref.append(outs)
+        integ.sync()
+        got = [_outs(o, dev) for _, o in ents]
+        b = integ.batch([(m, o, g) for (m, o), g in zip(ents, got)], tune=True)
+        b.run()
+        integ.sync()
+        info = b.info()
+        b.close()
+    assert info["samples"] == sum(W.samples_of(o) for _, o in ents)
+    for k, (r, g) in enumerate(zip(ref, got)):
+        for key, t in r.items():
+            if t is None:
+                continue
+            e = rel_err(g[key].cpu().numpy(), t.cpu().numpy())
+            assert e <= 1e-5, (k, key, e)
+            assert t.abs().max().item() > 0 or key == "fd"
