@@ -50,6 +50,7 @@ SIGNATURES = {
     "hxg_synchrotron": (C.c_int, [C.c_int, C.c_uint64, _dp, _dp]),
     "hxg_download_grid": (C.c_int, [_h, C.c_int, _dp, _dp, _dp]),
     "hxg_write_grid_multi": (C.c_int, [_h, C.c_int, C.POINTER(abi.Obs), C.POINTER(_vp)]),
+    "hxg_write_grid_multi_host": (C.c_int, [_h, C.c_int, C.POINTER(abi.Obs), C.POINTER(_vp)]),
     "hxg_shell_integrate_multi_device": (C.c_int, [_h, C.c_int, C.POINTER(abi.Obs), C.c_uint32,
                                                    C.c_uint32, C.c_uint32, _vp, _vp, _vp,
                                                    C.POINTER(_vp)]),

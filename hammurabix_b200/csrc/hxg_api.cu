@@ -1606,6 +1606,45 @@ int hxg_write_grid_multi(hxg_handle *h, int npass, const hxg_obs_t *obs, double 
   return HXG_OK;
 }
 
+int hxg_write_grid_multi_host(hxg_handle *h, int npass, const hxg_obs_t *obs,
+                              double *const *outs) {
+  if (!h) return HXG_ERR_INVALID;
+  if (npass < 1 || !obs || !outs) return fail(h, HXG_ERR_INVALID, "bad pass list");
+  cudaSetDevice(h->device);
+  // device maps for every requested output, one allocation
+  const auto count = [](const hxg_obs_t &o, int j) -> size_t {
+    const bool on[5] = {o.do_dm != 0, o.do_fd != 0, o.do_sync != 0, o.do_sync != 0,
+                        o.do_sync != 0};
+    const uint32_t ns[5] = {o.nside_dm, o.nside_fd, o.nside_sync, o.nside_sync, o.nside_sync};
+    return on[j] ? npix_of(ns[j]) : 0;
+  };
+  size_t total = 0;
+  for (int k = 0; k < npass; ++k)
+    for (int j = 0; j < 5; ++j) {
+      if (count(obs[k], j) && !outs[5 * k + j])
+        return fail(h, HXG_ERR_INVALID, "pass %d: output %d requested but NULL", k, j);
+      total += count(obs[k], j);
+    }
+  int st = ensure(h, h->out[0], std::max<size_t>(total, 1) * sizeof(double));
+  if (st != HXG_OK) return st;
+  std::vector<double *> dev(5 * npass, nullptr);
+  double *base = static_cast<double *>(h->out[0].p);
+  for (int k = 0, off = 0; k < npass; ++k)
+    for (int j = 0; j < 5; ++j)
+      if (const size_t c = count(obs[k], j)) {
+        dev[5 * k + j] = base + off;
+        off += (int)c;
+      }
+  if ((st = hxg_write_grid_multi(h, npass, obs, dev.data())) != HXG_OK) return st;
+  for (int k = 0; k < npass; ++k)
+    for (int j = 0; j < 5; ++j)
+      if (const size_t c = count(obs[k], j))
+        HXG_CK(cudaMemcpyAsync(outs[5 * k + j], dev[5 * k + j], c * sizeof(double),
+                               cudaMemcpyDeviceToHost, h->stream));
+  HXG_CK(cudaStreamSynchronize(h->stream));
+  return HXG_OK;
+}
+
 int hxg_shell_integrate_device(hxg_handle *h, const hxg_obs_t *o, uint32_t shell,
                                uint32_t shard, uint32_t nshards, const double *d_fd,
                                double *d_tmp_dm, double *d_tmp_fd, double *d_tmp_is,

@@ -32,6 +32,7 @@ inline void check(int st, hxg_handle *h, const char *what) {
 // (Pipeline::assemble_obs calls write_grid once per <sync> entry).
 struct DeviceState {
   hxg_handle *h = nullptr;
+  int precision = HXG_FP64;
   const void *uploaded[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   ~DeviceState() {
     if (h) hxg_destroy(h);
@@ -45,6 +46,7 @@ inline DeviceState &state() {
     const int prec = (p && std::string(p) == "fp32c") ? HXG_FP32C : HXG_FP64;
     const char *d = std::getenv("HAMMURABIX_DEVICE");
     check(hxg_create(d ? std::atoi(d) : 0, prec, &s.h), nullptr, "hxg_create");
+    s.precision = prec;
   }
   return s;
 }

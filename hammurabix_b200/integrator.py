@@ -138,23 +138,23 @@ class Integrator:
         _lib.check(self._lib.hxg_sync(self._h), self._h)
 
     def write_grid_multi(self, passes):
-        """Host-side hxg_write_grid_multi: passes is a list of Obs; returns
-        one dict dm/fd/is/qs/us of float64 numpy maps per pass (None where
-        the pass writes no such map).  The device maps are torch tensors
-        written on the handle's stream; the call waits for it."""
-        import torch
-        dev = torch.device("cuda", self.device)
+        """hxg_write_grid_multi_host: passes is a list of Obs; returns one
+        dict dm/fd/is/qs/us of float64 numpy maps per pass (None where the
+        pass writes no such map)."""
         keys = ("dm", "fd", "is", "qs", "us")
-        dev_maps = []
-        for o in passes:
+        n = len(passes)
+        obs = (abi.Obs * n)(*passes)
+        out, ptrs = [], (C.c_void_p * (5 * n))()
+        for k, o in enumerate(passes):
             ndm, nfd, nsy = abi.obs_output_sizes(o)
-            dev_maps.append([torch.empty(n, dtype=torch.float64, device=dev) if n else None
-                             for n in (ndm, nfd, nsy, nsy, nsy)])
-        torch.cuda.synchronize(dev)           # allocations settled before the library writes
-        self.write_grid_multi_device(list(zip(passes, dev_maps)))
-        self.sync()
-        return [{k: (t.cpu().numpy() if t is not None else None) for k, t in zip(keys, maps)}
-                for maps in dev_maps]
+            maps = {key: (np.zeros(c) if c else None)
+                    for key, c in zip(keys, (ndm, nfd, nsy, nsy, nsy))}
+            for j, key in enumerate(keys):
+                if maps[key] is not None:
+                    ptrs[5 * k + j] = maps[key].ctypes.data
+            out.append(maps)
+        _lib.check(self._lib.hxg_write_grid_multi_host(self._h, n, obs, ptrs), self._h)
+        return out
 
     def write_grid_multi_device(self, passes):
         """Several frequency passes at once (hxg_write_grid_multi): passes is

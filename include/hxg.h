@@ -312,6 +312,10 @@ int hxg_sync(hxg_handle *h);
  * handle's stream.  No counterpart in the reference.                       */
 int hxg_write_grid_multi(hxg_handle *h, int npass, const hxg_obs_t *obs,
                          double *const *d_outs);
+/* Same with host output buffers (outs[5k..5k+4] of pass k, NULL where the
+ * pass writes no such map); synchronous.                                 */
+int hxg_write_grid_multi_host(hxg_handle *h, int npass, const hxg_obs_t *obs,
+                              double *const *outs);
 
 /* ---- one shell at a time, over a shard of its pixels ---------------------
  * The two halves of one iteration of write_grid's shell loop

@@ -100,3 +100,17 @@ def test_mixed_geometry_and_fp64(fields32, dev_stream):
         ig = _integ(prec, fields32, W.grid_models(), dev, stream)
         _compare(ig, passes, dev)
         ig.close()
+
+
+def test_passes_with_their_own_output_nsides(fields32, dev_stream):
+    """One fused group whose passes write maps at different Nsides (the
+    drop-in test's XML has 0.408 GHz at Nside 16 and 23 GHz at Nside 8):
+    the merges go out per output Nside."""
+    dev, stream = dev_stream
+    ig = _integ("fp32c", fields32, W.grid_models(), dev, stream)
+    tmpl = W.make_obs([4, 8, 16], 20.0, 0.05, freq_ghz=0.408, nside_out=16)
+    passes = W.frequency_passes(tmpl, [0.408, 23.0, 5.0])
+    passes[1].nside_sync = 8
+    passes[2].nside_sync = 32
+    _compare(ig, passes, dev)
+    ig.close()
