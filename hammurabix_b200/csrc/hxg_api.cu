@@ -1488,7 +1488,7 @@ int fused_shell(hxg_handle *h, const hxg_obs_t *o, uint32_t s, uint32_t shard, u
   P.log2_chunks = hpx_ilog2((uint64_t)C);
   if (local == 0) return HXG_OK;
   const uint64_t warps = (local + (32 / C) - 1) / (32 / C);
-  const unsigned threads = 256;
+  const unsigned threads = HXG_FP32C_MULTI_THREADS;
   const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (h->timing) {

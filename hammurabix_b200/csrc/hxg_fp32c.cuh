@@ -486,11 +486,8 @@ shell_fp32c_kernel(const ShellLaunch P) {
 
 // NF frequency passes in one traversal of the shell (2 resident blocks: the
 // per-pass Q/U sums and phase constants take registers).
-#ifndef HXG_FP32C_MULTI_MIN_BLOCKS
-#define HXG_FP32C_MULTI_MIN_BLOCKS 2
-#endif
 template <int NG, bool kExt, int NF>
-__global__ void __launch_bounds__(256, HXG_FP32C_MULTI_MIN_BLOCKS)
+__global__ void __launch_bounds__(HXG_FP32C_MULTI_THREADS, HXG_FP32C_MULTI_MIN_BLOCKS)
 shell_fp32c_multi_kernel(const ShellLaunch P, const FreqSet<NF> Fq) {
   fp32c_tile<NG, kExt, NF>(P, Fq, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
                            threadIdx.x & 31);

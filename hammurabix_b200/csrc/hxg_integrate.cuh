@@ -77,6 +77,18 @@ struct ShellLaunch {
 // phase scale, emissivity scales, temp_convert and I/Q/U shell maps.  The
 // positions, field samples, emissivity weights, DM and FD of a sample do not
 // depend on the frequency and are computed once for all NF passes.
+// Launch shape of the fused-frequency shell kernel: threads per block and
+// the resident blocks per SM its register budget is cut for.  128 x 5
+// (96 registers, a few spilled) keeps 20 warps per SM and ran config 3 in
+// 91.3 ms against 92.8 ms at 256 x 2 (128 registers) and 97.2 ms at
+// 128 x 6 (80 registers, more spills).
+#ifndef HXG_FP32C_MULTI_THREADS
+#define HXG_FP32C_MULTI_THREADS 128
+#endif
+#ifndef HXG_FP32C_MULTI_MIN_BLOCKS
+#define HXG_FP32C_MULTI_MIN_BLOCKS 5
+#endif
+
 template <int NF>
 struct FreqSet {
   double lambda2[NF];   // (c/nu)^2
