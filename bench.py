@@ -370,7 +370,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="config3", choices=sorted(WORKLOADS))
     ap.add_argument("--fp64-steps", type=int, default=1)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=2)
     ap.add_argument("--batch-steps", type=int, default=2)
@@ -546,31 +546,57 @@ def main():
             p.copy_(t)
         hosts = [p.numpy() for p in pinned]
         keys = ("dm", "fd", "is", "qs", "us")
-        pinned_out = [{k: torch.empty(npx, dtype=torch.float64, pin_memory=True).numpy()
-                       for k in keys} for _ in passes]
-        ige = Integrator("fp32c", device=local)
-        ige.set_stream(stream.cuda_stream)
-        ige.set_models(models)
-        dev_out = outputs()
 
-        def e2e_step():
-            # grids from pinned host memory, the step on the device (the same
-            # fused or split passes as the product path), maps back to pinned
-            # host memory
-            ige.upload_grid(abi.HXG_FIELD_BRND, desc, hosts[:3])
-            ige.upload_grid(abi.HXG_FIELD_TEREG, desc, hosts[3:])
-            step(ige, dev_out)
-            for o, m, po in zip(passes, dev_out, pinned_out):
+        def e2e_integ(s):
+            ig_ = Integrator("fp32c", device=local)
+            ig_.set_stream(s.cuda_stream)
+            ig_.set_models(models)
+            return ig_
+
+        def read_back(outs, pinned_out):
+            for o, m, po in zip(passes, outs, pinned_out):
                 for k, t in zip(keys, sel(o, m)):
                     if t is not None:
                         torch.from_numpy(po[k]).copy_(t, non_blocking=True)
-            torch.cuda.synchronize(dev)
 
-        e2e_step()
+        def upload(ig_):
+            ig_.upload_grid(abi.HXG_FIELD_BRND, desc, hosts[:3])
+            ig_.upload_grid(abi.HXG_FIELD_TEREG, desc, hosts[3:])
+
+        if shard:
+            # every rank takes the same collective steps in the same order:
+            # one handle, one stream, steps one after another
+            e2e_streams = [stream]
+        else:
+            # two handles on two streams: step k+1's grids cross PCIe (the
+            # upload returns when its copies are done) while step k runs on
+            # the other stream, and step k's maps come back while step k+1
+            # runs; every step still uploads its own grids and reads back
+            # its own maps inside the timed region
+            e2e_streams = [stream, torch.cuda.Stream(dev)]
+        iges = [e2e_integ(s) for s in e2e_streams]
+        e2e_outs = [outputs() for _ in iges]
+        pinned_outs = [[{k: torch.empty(npx, dtype=torch.float64, pin_memory=True).numpy()
+                         for k in keys} for _ in passes] for _ in iges]
+
+        def e2e_run(nsteps):
+            npipe = len(iges)
+            upload(iges[0])
+            for k in range(nsteps):
+                a, b = k % npipe, (k + 1) % npipe
+                with torch.cuda.stream(e2e_streams[a]):
+                    step(iges[a], e2e_outs[a])
+                    read_back(e2e_outs[a], pinned_outs[a])
+                if k + 1 < nsteps:
+                    e2e_streams[b].synchronize()    # step k-1 (or k) done, maps home
+                    upload(iges[b])
+            for s in e2e_streams:
+                s.synchronize()
+
+        e2e_run(2)
         barrier()
         te0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            e2e_step()
+        e2e_run(args.e2e_steps)
         barrier()
         te = max_over_ranks((time.perf_counter() - te0) / args.e2e_steps)
         h2d = sum(h.nbytes for h in hosts)
@@ -578,9 +604,12 @@ def main():
                        + 3 * abi.npix(o.nside_sync)) for o in passes)
         e2e = {"value": (1 if shard else ws) * samples_step / te, "unit": UNIT,
                "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "ms_per_step": te * 1e3}
-        ige.close()
-        del pinned, hosts
+               "d2h_bytes_per_step": d2h, "ms_per_step": te * 1e3,
+               "overlap": ("two handles on two streams: step k+1's upload and step k-1's "
+                           "read-back overlap step k") if len(iges) > 1 else "none"}
+        for ig_ in iges:
+            ig_.close()
+        del pinned, hosts, pinned_outs
         log(f"[rank {rank}] e2e: {te * 1e3:.1f} ms/step")
 
     # ---- adjoint / forward cost on the config-4 workload (FP64 form) -------

@@ -64,6 +64,9 @@ struct hxg_handle {
   Slot slots[5];
   std::vector<Group> groups;
   bool groups_dirty = true;
+  // bumped whenever a grid slot or a group's record array moves to new
+  // device memory; a batch made before that refuses to run
+  uint64_t layout_gen = 0;
   bool have_mask = false;
   uint32_t mask_nside = 0;
   std::vector<double> mask_host;
@@ -188,21 +191,23 @@ void free_groups(hxg_handle *h) {
 }
 
 // Pack every active grid slot into per-geometry 4-component record arrays.
+// New values in the same slots and geometries are packed into the record
+// arrays already there, so plans that hold their addresses stay valid.
 int build_groups(hxg_handle *h) {
   if (!h->groups_dirty) return HXG_OK;
-  free_groups(h);
   bool act[4];
   active_slots(h->models, act);
+  std::vector<Group> next;
   for (int s = 0; s < 4; ++s) {
     if (!act[s]) continue;
     if (!h->slots[s].present)
       return fail(h, HXG_ERR_STATE, "model reads grid slot %d but no grid was uploaded", s);
     Group *grp = nullptr;
-    for (auto &g : h->groups)
+    for (auto &g : next)
       if (same_geometry(g.desc, h->slots[s].desc)) grp = &g;
     if (!grp) {
-      h->groups.emplace_back();
-      grp = &h->groups.back();
+      next.emplace_back();
+      grp = &next.back();
       grp->desc = h->slots[s].desc;
       grp->n = h->slots[s].n;
     }
@@ -213,13 +218,33 @@ int build_groups(hxg_handle *h) {
     else
       list[1] = s;
   }
-  if (h->groups.size() > (size_t)kMaxGroups)
+  if (next.size() > (size_t)kMaxGroups)
     return fail(h, HXG_ERR_UNSUPPORTED, "more than %d grid geometries", kMaxGroups);
+  bool same = next.size() == h->groups.size();
+  for (size_t i = 0; same && i < next.size(); ++i) {
+    const Group &a = next[i], &b = h->groups[i];
+    same = b.rec && a.n == b.n && same_geometry(a.desc, b.desc) &&
+           std::memcmp(a.b_slots, b.b_slots, sizeof(a.b_slots)) == 0 &&
+           std::memcmp(a.t_slots, b.t_slots, sizeof(a.t_slots)) == 0;
+  }
+  if (same) {
+    for (size_t i = 0; i < next.size(); ++i) next[i].rec = h->groups[i].rec;
+    h->groups.clear();
+  } else {
+    free_groups(h);
+    ++h->layout_gen;
+  }
+  h->groups = std::move(next);
   const bool fp32 = h->precision == HXG_FP32C;
   const size_t esz = fp32 ? sizeof(float) : sizeof(double);
   for (auto &g : h->groups) {
-    cudaError_t e = cudaMalloc(&g.rec, g.n * 4 * esz);
-    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc(grid records)");
+    if (!g.rec) {
+      cudaError_t e = cudaMalloc(&g.rec, g.n * 4 * esz);
+      if (e != cudaSuccess) {
+        free_groups(h);
+        return cuda_fail(h, e, "cudaMalloc(grid records)");
+      }
+    }
     const double *b0[3] = {nullptr, nullptr, nullptr};
     const double *b1[3] = {nullptr, nullptr, nullptr};
     if (g.b_slots[0] >= 0)
@@ -755,10 +780,11 @@ int slot_prepare(hxg_handle *h, int field, const hxg_grid_desc_t *g, size_t *n_o
   const int ncomp = (field == HXG_FIELD_BREG || field == HXG_FIELD_BRND) ? 3 : 1;
   Slot &S = h->slots[field];
   const size_t n = (size_t)g->nx * g->ny * g->nz * (field == HXG_FIELD_CRE ? g->nE : 1);
-  if (S.present && S.n != n) {
+  if (S.n != n && (S.d[0] || S.d[1] || S.d[2])) {
     for (auto &p : S.d)
       if (p) cudaFree(p);
     S.d[0] = S.d[1] = S.d[2] = nullptr;
+    ++h->layout_gen;
   }
   S.present = false;
   for (int k = 0; k < ncomp; ++k) {
@@ -2151,6 +2177,7 @@ struct hxg_batch {
   unsigned long long zero_blocks = 0;
   unsigned level_blocks[3] = {0, 0, 0};
   int graph_kernels = 0;  // kernels one run of the graph launches
+  uint64_t layout_gen = 0;  // the handle's layout_gen the graph was made for
   cudaGraphExec_t exec = nullptr;
 };
 
@@ -2439,6 +2466,7 @@ int hxg_batch_create(hxg_handle *h, int n, const hxg_batch_entry_t *entries,
   if ((st = build_groups(h)) != HXG_OK) return st;
   hxg_batch *b = new hxg_batch();
   b->h = h;
+  b->layout_gen = h->layout_gen;
   b->e.assign(entries, entries + n);
   b->fp32 = h->precision == HXG_FP32C;
   b->ngroups = (int)h->groups.size();
@@ -2554,6 +2582,14 @@ int hxg_batch_run(hxg_batch *b) {
   if (!b || !b->exec) return HXG_ERR_INVALID;
   hxg_handle *h = b->h;
   cudaSetDevice(h->device);
+  // grids uploaded since the last run are packed into the same record
+  // arrays; a new geometry or set of grid fields moves them
+  const int st = build_groups(h);
+  if (st != HXG_OK) return st;
+  if (b->layout_gen != h->layout_gen)
+    return fail(h, HXG_ERR_STATE,
+                "the handle's grids changed geometry or fields since hxg_batch_create; "
+                "create the batch again");
   HXG_CK(cudaGraphLaunch(b->exec, h->stream));
   h->launch_count += b->graph_kernels;
   return HXG_OK;

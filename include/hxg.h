@@ -415,7 +415,10 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *obs,
  *  - tune != 0: the launch shapes (lanes per pixel x tiles per fetch) are
  *    timed once in hxg_batch_create and the fastest is kept;
  *  - hxg_batch_run launches the graph on the handle's stream and does not
- *    synchronise; the entries' host data are not read again.             */
+ *    synchronise; the entries' host data are not read again;
+ *  - grids uploaded to the handle after hxg_batch_create with the same
+ *    geometries are used by the next run; if the handle's grids change
+ *    geometry or fields, hxg_batch_run returns HXG_ERR_STATE.            */
 typedef struct {
   hxg_models_t models;
   hxg_obs_t obs;

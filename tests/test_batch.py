@@ -138,3 +138,48 @@ def test_batch_fuses_the_frequencies_of_a_parameter_set(fields32):
             e = rel_err(g[key].cpu().numpy(), t.cpu().numpy())
             assert e <= 1e-5, (k, key, e)
             assert t.abs().max().item() > 0 or key == "fd"
+
+
+def test_batch_follows_new_grids_and_refuses_a_new_geometry(fields32):
+    """Grids uploaded after hxg_batch_create with the same geometry are
+    packed into the record arrays the graph reads: the next run gives the
+    maps of the new grids.  A grid of another geometry moves the records,
+    and the run is refused with HXG_ERR_STATE instead of reading them."""
+    dev = torch.device("cuda", 0)
+    rng = np.random.Generator(np.random.PCG64(12))
+    ents = _entries(rng, 3)
+    bx, by, bz, ne = (torch.tensor(np.asarray(a, dtype=np.float64).reshape(-1), device=dev)
+                      for a in fields32)
+    with I.Integrator("fp64") as integ:
+        integ.set_models(ents[0][0])
+        integ.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(32), [bx, by, bz])
+        integ.upload_grid_device(abi.HXG_FIELD_TEREG, W.grid_desc(32), [ne])
+        got = [_outs(o, dev) for _, o in ents]
+        b = integ.batch([(m, o, g) for (m, o), g in zip(ents, got)])
+        b.run()
+        # new values, same geometry: half the field, twice the density
+        integ.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(32),
+                                 [0.5 * bx, 0.5 * by, 0.5 * bz])
+        integ.upload_grid_device(abi.HXG_FIELD_TEREG, W.grid_desc(32), [2.0 * ne])
+        b.run()
+        integ.sync()
+        ref = []
+        for m, o in ents:
+            integ.set_models(m)
+            outs = _outs(o, dev)
+            integ.write_grid_device(o, outs["dm"], outs["fd"], outs["is"], outs["qs"], outs["us"])
+            ref.append(outs)
+        integ.sync()
+        for k, (r, g) in enumerate(zip(ref, got)):
+            for key, t in r.items():
+                if t is None:
+                    continue
+                e = rel_err(g[key].cpu().numpy(), t.cpu().numpy())
+                assert e <= 1e-10, (k, key, e)
+        small = [t.reshape(32, 32, 32)[::2, ::2, ::2].contiguous().reshape(-1)
+                 for t in (bx, by, bz)]
+        integ.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(16), small)
+        with pytest.raises(_lib.HxgError) as e:
+            b.run()
+        assert e.value.status == abi.HXG_ERR_STATE
+        b.close()
