@@ -7,7 +7,10 @@ Integrator::write_grid (source/integrator/integrator.cc:23-134) over the C ABI.
     maps = integ.write_grid(obs)                  # dict dm/fd/is/qs/us (numpy)
 
 Device-resident inputs and outputs (torch CUDA tensors) go through
-``upload_grid_device`` and ``write_grid_device``.
+``upload_grid_device`` and ``write_grid_device``.  Those calls are ordered
+like torch ops on torch's current stream: the library's stream waits for
+the work queued there before the call, and torch's stream waits for the
+library's launches after it.
 """
 import ctypes as C
 import os
@@ -27,6 +30,7 @@ class Integrator:
         _lib.check(self._lib.hxg_create(int(device), PRECISIONS[precision], C.byref(h)))
         self._h = h
         self.device = device
+        self._stream = None   # torch stream object of the handle's stream
 
     def close(self):
         if getattr(self, "_h", None):
@@ -53,6 +57,31 @@ class Integrator:
         """Launch on a CUDA stream (integer cudaStream_t, e.g.
         torch.cuda.current_stream().cuda_stream); 0 = the handle's own."""
         _lib.check(self._lib.hxg_set_stream(self._h, C.c_void_p(stream_ptr or None)), self._h)
+        self._stream = None
+        if stream_ptr:
+            import torch
+            self._stream = torch.cuda.ExternalStream(
+                stream_ptr, device=torch.device("cuda", self.device))
+
+    def _ordered(self, call):
+        """Run call() (a C entry point returning a status) that reads or
+        writes torch CUDA tensors, ordered with torch's current stream.  The
+        first such call on a handle without a stream of the caller's gives
+        the handle a torch stream, so both ends can wait on events."""
+        import torch
+        if self._stream is None:
+            s = torch.cuda.Stream(self.device)
+            _lib.check(self._lib.hxg_set_stream(self._h, C.c_void_p(s.cuda_stream)), self._h)
+            self._stream = s
+        cur = torch.cuda.current_stream(self.device)
+        same = cur.cuda_stream == self._stream.cuda_stream
+        if not same:
+            self._stream.wait_stream(cur)
+        try:
+            _lib.check(call(), self._h)
+        finally:
+            if not same:
+                cur.wait_stream(self._stream)
 
     def upload_grid(self, field, desc, comps):
         """Host FP64 SoA arrays in the Grid_* layout (x-major, z fastest)."""
@@ -64,8 +93,8 @@ class Integrator:
     def upload_grid_device(self, field, desc, comps):
         """Device FP64 SoA arrays (torch CUDA float64 tensors, contiguous)."""
         ptrs = [C.c_void_p(t.data_ptr()) for t in comps] + [None] * (3 - len(comps))
-        _lib.check(self._lib.hxg_upload_grid_device(self._h, int(field), C.byref(desc),
-                                                    *ptrs), self._h)
+        self._ordered(lambda: self._lib.hxg_upload_grid_device(self._h, int(field),
+                                                               C.byref(desc), *ptrs))
 
     def upload_grid_file(self, field, desc, path):
         """Load a grid from the reference's binary grid file
@@ -131,8 +160,8 @@ class Integrator:
         """Asynchronous variant writing into device buffers (torch CUDA
         float64 tensors) on the handle's stream."""
         ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
-        _lib.check(self._lib.hxg_write_grid_device(
-            self._h, C.byref(obs), ptr(dm), ptr(fd), ptr(is_), ptr(qs), ptr(us)), self._h)
+        self._ordered(lambda: self._lib.hxg_write_grid_device(
+            self._h, C.byref(obs), ptr(dm), ptr(fd), ptr(is_), ptr(qs), ptr(us)))
 
     def sync(self):
         _lib.check(self._lib.hxg_sync(self._h), self._h)
@@ -167,7 +196,7 @@ class Integrator:
         for k, (_, maps) in enumerate(passes):
             for j, t in enumerate(maps):
                 ptrs[5 * k + j] = t.data_ptr() if t is not None else None
-        _lib.check(self._lib.hxg_write_grid_multi(self._h, n, obs, ptrs), self._h)
+        self._ordered(lambda: self._lib.hxg_write_grid_multi(self._h, n, obs, ptrs))
 
     # ---- one shell over a shard of its pixels ---------------------------------
     def shell_integrate_device(self, obs, shell, shard, nshards, fd, tmp):
@@ -176,9 +205,9 @@ class Integrator:
         at least 12 nside_shell^2 elements, or None where obs needs none);
         fd = the accumulated FD output (hxg_shell_integrate_device)."""
         ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
-        _lib.check(self._lib.hxg_shell_integrate_device(
+        self._ordered(lambda: self._lib.hxg_shell_integrate_device(
             self._h, C.byref(obs), int(shell), int(shard), int(nshards), ptr(fd),
-            *(ptr(t) for t in tmp)), self._h)
+            *(ptr(t) for t in tmp)))
 
     def shell_integrate_multi_device(self, passes, shell, shard, nshards, fd, tmp_dm, tmp_fd,
                                      tmp_iqu):
@@ -188,17 +217,17 @@ class Integrator:
         obs = (abi.Obs * n)(*passes)
         iqu = (C.c_void_p * (3 * n))(*[t.data_ptr() for maps in tmp_iqu for t in maps])
         ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
-        _lib.check(self._lib.hxg_shell_integrate_multi_device(
+        self._ordered(lambda: self._lib.hxg_shell_integrate_multi_device(
             self._h, n, obs, int(shell), int(shard), int(nshards), ptr(fd), ptr(tmp_dm),
-            ptr(tmp_fd), iqu), self._h)
+            ptr(tmp_fd), iqu))
 
     def shell_merge_device(self, obs, shell, tmp, outs):
         """Accumulate shell maps tmp into the pass outputs outs = [dm, fd, is,
         qs, us] (hxg_shell_merge_device)."""
         ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
-        _lib.check(self._lib.hxg_shell_merge_device(
+        self._ordered(lambda: self._lib.hxg_shell_merge_device(
             self._h, C.byref(obs), int(shell), *(ptr(t) for t in tmp),
-            *(ptr(t) for t in outs)), self._h)
+            *(ptr(t) for t in outs)))
 
     # ---- adjoint -----------------------------------------------------------
     def set_checkpointing(self, enable=True):
@@ -212,9 +241,9 @@ class Integrator:
         grad_ne (one tensor) with dL/d(parameters) and dL/d(grid values)."""
         ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
         gb = list(grad_b) if grad_b is not None else [None, None, None]
-        _lib.check(self._lib.hxg_adjoint_device(
+        self._ordered(lambda: self._lib.hxg_adjoint_device(
             self._h, C.byref(obs), ptr(g_dm), ptr(g_fd), ptr(g_is), ptr(g_qs), ptr(g_us),
-            ptr(grad_params), ptr(gb[0]), ptr(gb[1]), ptr(gb[2]), ptr(grad_ne)), self._h)
+            ptr(grad_params), ptr(gb[0]), ptr(gb[1]), ptr(gb[2]), ptr(grad_ne)))
 
     # ---- batched forward ---------------------------------------------------
     def batch(self, entries, tune=False):
@@ -271,11 +300,11 @@ class Batch:
                     self._keep.append(t)
                     setattr(arr[k], field, t.data_ptr())
         self._b = C.c_void_p()
-        _lib.check(self._lib.hxg_batch_create(integ._h, len(entries), arr, int(bool(tune)),
-                                              C.byref(self._b)), integ._h)
+        integ._ordered(lambda: self._lib.hxg_batch_create(integ._h, len(entries), arr,
+                                                          int(bool(tune)), C.byref(self._b)))
 
     def run(self):
-        _lib.check(self._lib.hxg_batch_run(self._b), self._integ._h)
+        self._integ._ordered(lambda: self._lib.hxg_batch_run(self._b))
 
     def info(self):
         lanes, grain, tried = C.c_int(), C.c_int(), C.c_int()

@@ -35,9 +35,9 @@ def shell_maps_needed(obs):
 def write_grid_sharded(integ, obs, outs, tmp, rank, world, reduce_sum):
     """One pass on this rank.
 
-    integ: an Integrator whose stream (Integrator.set_stream) is the caller's
-    current torch stream, a non-null one: the zeroing and the reductions run
-    there, between the library's launches;
+    integ: an Integrator; its device calls are ordered with the caller's
+    current torch stream, where the zeroing and the reductions run (giving
+    it that stream with Integrator.set_stream saves the event waits);
     outs: dict of the pass outputs (device tensors, the requested ones);
     tmp: dict of shell-map buffers of 12 max(nside_shell)^2 doubles;
     reduce_sum(t): in-place sum of t over the ranks, in stream order."""

@@ -157,7 +157,8 @@ def test_batch_follows_new_grids_and_refuses_a_new_geometry(fields32):
         got = [_outs(o, dev) for _, o in ents]
         b = integ.batch([(m, o, g) for (m, o), g in zip(ents, got)])
         b.run()
-        # new values, same geometry: half the field, twice the density
+        # new values, same geometry: half the field, twice the density (made
+        # on torch's stream; the upload is ordered after them)
         integ.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(32),
                                  [0.5 * bx, 0.5 * by, 0.5 * bz])
         integ.upload_grid_device(abi.HXG_FIELD_TEREG, W.grid_desc(32), [2.0 * ne])
