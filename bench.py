@@ -636,8 +636,8 @@ def main():
     samples_per_launch = ksamples / max(klaunch, 1)
     achieved = samples_per_launch * BYTES_PER_SAMPLE["fp32c"] / per_launch_s / 1e9
     fused = len(passes) in (2, 3)
-    kname = (f"hxg::shell_fp32c_multi_kernel<1,false,{len(passes)}>" if fused
-             else "hxg::shell_fp32c_kernel<1,false>")
+    kname = (f"hxg::shell_fp32c_multi_kernel<1,false,{len(passes)},true>" if fused
+             else "hxg::shell_fp32c_kernel<1,false,true>")
     tps = traffic_per_sample("shell_fp32c_multi_config3.md" if fused
                              else "shell_fp32c_config3.md")
     traffic = (tps * samples_per_launch) if tps else None

@@ -707,6 +707,16 @@ int build_launch(hxg_handle *h, const hxg_models_t &m, const hxg_obs_t &o,
     F.ex_n0 = D.tex_n0;
     F.ex_irn = 1. / D.tex_rs;
     F.ex_ihn = 1. / D.tex_hs;
+    F.r2min = P.gc_r_min * P.gc_r_min;
+    F.r2max = P.gc_r_max * P.gc_r_max;
+    F.rc2_hi = 400. * D.kpc * D.kpc;
+    F.rc2_lo = 9. * D.kpc * D.kpc;
+    F.sp_sinf = float(D.sp_sin);
+    F.sp_cosf = float(D.sp_cos);
+    F.cre_ir0 = float(1. / D.cre_r0);
+    F.cre_2iz0 = float(2. / D.cre_z0);
+    F.cre_R0 = float(D.cre_R0);
+    F.pe = float(P.em_pe);
   } else {
     P.fd_fore = fdfore;
   }
@@ -720,6 +730,9 @@ int build_launch(hxg_handle *h, const hxg_models_t &m, const hxg_obs_t &o,
     D.ny = (int)G.desc.ny;
     D.nz = (int)G.desc.nz;
     D.has_b = G.b_slots[0] >= 0;
+    D.gmax[0] = (double)(G.desc.nx - 1);
+    D.gmax[1] = (double)(G.desc.ny - 1);
+    D.gmax[2] = (double)(G.desc.nz - 1);
     D.lo[0] = G.desc.x_min * L;
     D.lo[1] = G.desc.y_min * L;
     D.lo[2] = G.desc.z_min * L;
@@ -2123,6 +2136,9 @@ int hxg_read_grid(hxg_handle *h, int field, uint64_t n, const double *pos,
   D.nx = (int)G->desc.nx;
   D.ny = (int)G->desc.ny;
   D.nz = (int)G->desc.nz;
+  D.gmax[0] = (double)(G->desc.nx - 1);
+  D.gmax[1] = (double)(G->desc.ny - 1);
+  D.gmax[2] = (double)(G->desc.nz - 1);
   D.lo[0] = G->desc.x_min * L;
   D.lo[1] = G->desc.y_min * L;
   D.lo[2] = G->desc.z_min * L;
@@ -2178,6 +2194,7 @@ struct hxg_batch {
   unsigned level_blocks[3] = {0, 0, 0};
   int graph_kernels = 0;  // kernels one run of the graph launches
   uint64_t layout_gen = 0;  // the handle's layout_gen the graph was made for
+  bool fast = false;        // every entry's models satisfy fast_models
   cudaGraphExec_t exec = nullptr;
 };
 
@@ -2375,15 +2392,18 @@ int batch_capture(hxg_batch *b) {
         B.nplans = b->nplans[k];
         B.grain = b->grain;
         B.counter = ctr + k;
-        e = hxg::launch_batch_level(s, b->fp32, b->ngroups, b->ext_any, B, b->level_blocks[0]);
+        e = hxg::launch_batch_level(s, b->fp32, b->ngroups, b->ext_any, b->fast, B,
+                                    b->level_blocks[0]);
       } else if (c == 1) {
         hxg::BatchLevelMulti<2> B{static_cast<const hxg::FusedPlan<2> *>(b->plans[k].p), tiles,
                                   b->nplans[k], b->grain, ctr + k};
-        e = hxg::launch_batch_level_multi(s, b->ngroups, b->ext_any, 2, &B, b->level_blocks[1]);
+        e = hxg::launch_batch_level_multi(s, b->ngroups, b->ext_any, b->fast, 2, &B,
+                                          b->level_blocks[1]);
       } else {
         hxg::BatchLevelMulti<3> B{static_cast<const hxg::FusedPlan<3> *>(b->plans[k].p), tiles,
                                   b->nplans[k], b->grain, ctr + k};
-        e = hxg::launch_batch_level_multi(s, b->ngroups, b->ext_any, 3, &B, b->level_blocks[2]);
+        e = hxg::launch_batch_level_multi(s, b->ngroups, b->ext_any, b->fast, 3, &B,
+                                          b->level_blocks[2]);
       }
     }
     if (e != cudaSuccess) break;
@@ -2545,12 +2565,21 @@ int hxg_batch_create(hxg_handle *h, int n, const hxg_batch_entry_t *entries,
     }
     if (b->ext_any && (st = upload_vec(h, b->ext, ext)) != HXG_OK) return bail(st);
   }
+  // the kFast kernels when every entry's models are among the grid workloads'
+  b->fast = true;
+  for (const hxg_batch_entry_t &E : b->e) {
+    ShellLaunch L;
+    uint64_t step;
+    if ((st = build_launch(h, E.models, E.obs, 0, L, step)) != HXG_OK) return bail(st);
+    L.ext = uses_ext(E.models) ? static_cast<const ExtModels *>(b->ext.p) : nullptr;
+    b->fast = b->fast && hxg::fast_models(L);
+  }
   int per_sm = 0;
-  cudaError_t ce = hxg::batch_level_occupancy(b->fp32, b->ngroups, b->ext_any, &per_sm);
+  cudaError_t ce = hxg::batch_level_occupancy(b->fp32, b->ngroups, b->ext_any, b->fast, &per_sm);
   if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "occupancy"));
   b->level_blocks[0] = (unsigned)std::max(1, per_sm) * (unsigned)h->sm_count;
   for (int nf = 2; nf <= 3 && b->fp32; ++nf) {
-    ce = hxg::batch_multi_occupancy(b->ngroups, b->ext_any, nf, &per_sm);
+    ce = hxg::batch_multi_occupancy(b->ngroups, b->ext_any, b->fast, nf, &per_sm);
     if (ce != cudaSuccess) return bail(cuda_fail(h, ce, "occupancy"));
     b->level_blocks[nf - 1] = (unsigned)std::max(1, per_sm) * (unsigned)h->sm_count;
   }

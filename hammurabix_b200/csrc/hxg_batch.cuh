@@ -52,7 +52,7 @@ __device__ __forceinline__ int batch_plan_of(const unsigned long long *tile_star
   return lo;
 }
 
-template <int NG, bool kExt, int NF>
+template <int NG, bool kExt, int NF, bool kFast>
 __device__ __forceinline__ void batch_multi_body(const BatchLevelMulti<NF> &B) {
   const int lane = threadIdx.x & 31;
   const unsigned long long total = B.tile_start[B.nplans];
@@ -66,18 +66,19 @@ __device__ __forceinline__ void batch_multi_body(const BatchLevelMulti<NF> &B) {
     for (unsigned long long t = t0; t < t1; ++t) {
       while (t >= B.tile_start[k + 1]) ++k;
       const FusedPlan<NF> &FP = B.plans[k];
-      fp32c_tile<NG, kExt, NF>(FP.P, FP.F, (long long)(t - B.tile_start[k]), lane);
+      fp32c_tile<NG, kExt, NF, kFast>(FP.P, FP.F, (long long)(t - B.tile_start[k]), lane);
     }
   }
 }
 
-template <int NG, bool kExt, int NF>
+// kFast: every plan's models satisfy fast_models.
+template <int NG, bool kExt, int NF, bool kFast>
 __global__ void __launch_bounds__(256, 2)
 batch_fp32c_multi_kernel(const BatchLevelMulti<NF> B) {
-  batch_multi_body<NG, kExt, NF>(B);
+  batch_multi_body<NG, kExt, NF, kFast>(B);
 }
 
-template <int NG, bool kFp32, bool kExt>
+template <int NG, bool kFp32, bool kExt, bool kFast>
 __device__ __forceinline__ void batch_level_body(const BatchLevel &B) {
   const int lane = threadIdx.x & 31;
   const unsigned long long total = B.tile_start[B.nplans];
@@ -99,25 +100,25 @@ __device__ __forceinline__ void batch_level_body(const BatchLevel &B) {
       const ShellLaunch &P = B.plans[k];
       const long long gw = (long long)(t - B.tile_start[k]);
       if (kFp32)
-        fp32c_tile<NG, kExt>(P, gw, lane);
+        fp32c_tile<NG, kExt, kFast>(P, gw, lane);
       else
-        fp64_tile<NG, false, kExt>(P, gw, lane);
+        fp64_tile<NG, false, kExt, kFast>(P, gw, lane);
     }
   }
 }
 
 // The launch blocks are read from global memory, which needs more live
 // registers than the single-launch kernel: 2 resident blocks per SM.
-template <int NG, bool kExt>
+template <int NG, bool kExt, bool kFast>
 __global__ void __launch_bounds__(256, 2)
 batch_fp32c_kernel(const BatchLevel B) {
-  batch_level_body<NG, true, kExt>(B);
+  batch_level_body<NG, true, kExt, kFast>(B);
 }
 
-template <int NG, bool kExt>
+template <int NG, bool kExt, bool kFast>
 __global__ void __launch_bounds__(256)
 batch_fp64_kernel(const BatchLevel B) {
-  batch_level_body<NG, false, kExt>(B);
+  batch_level_body<NG, false, kExt, kFast>(B);
 }
 
 // Map merges of one level: job j adds nmaps shell maps at nside_src into

@@ -76,6 +76,24 @@ __device__ __forceinline__ bool beyond_observer(T x, T y, T z,
 }
 
 // ---- regular magnetic field models (Breg::write_field overrides) ---------
+// The exponential-disk logarithmic spiral of the grid workloads (no
+// reference class: amplitude b0 exp(-(r - r_sun)/r_s) exp(-|z|/h_s), pitch
+// angle p, zero outside 3 kpc < r < 20 kpc).
+template <typename T>
+__device__ __forceinline__ V3<T> breg_spiral(const DevModels &m, T x, T y, T z,
+                                             const double p[3]) {
+  V3<T> b{T(0), T(0), T(0)};
+  const T r = sqrt(x * x + y * y);
+  if (outside_annulus<T>(r, p, m.kpc, 3., 20.)) return b;
+  const T cos_p = x / r, sin_p = y / r;
+  const T amp = T(m.sp_b0) * exp(-(r - T(m.sp_rsun)) / T(m.sp_rs)) *
+                exp(-fabs(z) / T(m.sp_hs));
+  const T sp = T(m.sp_sin), cp = T(m.sp_cos);
+  b.x = amp * (sp * cos_p - cp * sin_p);
+  b.y = amp * (sp * sin_p + cp * cos_p);
+  return b;
+}
+
 template <typename T>
 __device__ __forceinline__ V3<T> breg_model(const DevModels &m, T x, T y,
                                             T z, const double p[3]) {
@@ -119,33 +137,30 @@ __device__ __forceinline__ V3<T> breg_model(const DevModels &m, T x, T y,
       }
       return b;
     }
-    case kBregSpiral: {
-      const T r = sqrt(x * x + y * y);
-      if (outside_annulus<T>(r, p, m.kpc, 3., 20.)) return b;
-      const T cos_p = x / r, sin_p = y / r;
-      const T amp = T(m.sp_b0) * exp(-(r - T(m.sp_rsun)) / T(m.sp_rs)) *
-                    exp(-fabs(z) / T(m.sp_hs));
-      const T sp = T(m.sp_sin), cp = T(m.sp_cos);
-      b.x = amp * (sp * cos_p - cp * sin_p);
-      b.y = amp * (sp * sin_p + cp * cos_p);
-      return b;
-    }
+    case kBregSpiral:
+      return breg_spiral<T>(m, x, y, z, p);
     default:
       return b;
   }
 }
 
 // ---- regular thermal-electron models (TEreg::write_field overrides) ------
+// Exponential disk of the grid workloads (no reference class):
+// n0 exp(-r/r_s) exp(-|z|/h_s).
+template <typename T>
+__device__ __forceinline__ T tereg_expdisk(const DevModels &m, T x, T y, T z) {
+  const T r = sqrt(x * x + y * y);
+  return T(m.tex_n0) * exp(-r / T(m.tex_rs)) * exp(-fabs(z) / T(m.tex_hs));
+}
+
 template <typename T>
 __device__ __forceinline__ T tereg_model(const DevModels &m, T x, T y, T z,
                                         const double p[3]) {
   switch (m.tereg) {
     case kTeregUnif:  // tereg_unif.cc:6-12
       return beyond_observer<T>(x, y, z, p, m, m.teu_r0) ? T(0) : T(m.teu_n0);
-    case kTeregExpdisk: {
-      const T r = sqrt(x * x + y * y);
-      return T(m.tex_n0) * exp(-r / T(m.tex_rs)) * exp(-fabs(z) / T(m.tex_hs));
-    }
+    case kTeregExpdisk:
+      return tereg_expdisk<T>(m, x, y, z);
     default:
       return T(0);
   }
@@ -189,13 +204,16 @@ __device__ __forceinline__ T cre_index(const DevModels &m, T x, T y, T z) {
 }
 
 template <typename T>
+__device__ __forceinline__ T cre_profile_ana(const DevModels &m, T x, T y, T z) {
+  const T r = sqrt(x * x + y * y);
+  const T ch = cosh(z / T(m.cre_z0));
+  return exp((T(m.cre_R0) - r) / T(m.cre_r0)) * (T(1.) / (ch * ch));
+}
+
+template <typename T>
 __device__ __forceinline__ T cre_profile(const DevModels &m, T x, T y, T z,
                                         const double p[3]) {
-  if (m.cre == kCreAna) {
-    const T r = sqrt(x * x + y * y);
-    const T ch = cosh(z / T(m.cre_z0));
-    return exp((T(m.cre_R0) - r) / T(m.cre_r0)) * (T(1.) / (ch * ch));
-  }
+  if (m.cre == kCreAna) return cre_profile_ana<T>(m, x, y, z);
   return beyond_observer<T>(x, y, z, p, m, m.cre_unif_r0) ? T(0) : T(1);
 }
 
@@ -211,6 +229,7 @@ struct DevGridGroup {
   int nx, ny, nz, has_b;
   double lo[3];     // box minimum (working length units)
   double scale[3];  // (n - 1) / (max - min)
+  double gmax[3];   // n - 1: the grid coordinate of the upper box face
 };
 
 template <typename T>
@@ -251,11 +270,11 @@ __device__ __forceinline__ bool grid_coords(const DevGridGroup &g, double px,
                                             int &yl, int &zl, double &xd,
                                             double &yd, double &zd) {
   const double tx = (px - g.lo[0]) * g.scale[0];
-  if (!(tx > 0.) || tx >= double(g.nx - 1)) return false;
+  if (!(tx > 0.) || tx >= g.gmax[0]) return false;
   const double ty = (py - g.lo[1]) * g.scale[1];
-  if (!(ty > 0.) || ty >= double(g.ny - 1)) return false;
+  if (!(ty > 0.) || ty >= g.gmax[1]) return false;
   const double tz = (pz - g.lo[2]) * g.scale[2];
-  if (!(tz > 0.) || tz >= double(g.nz - 1)) return false;
+  if (!(tz > 0.) || tz >= g.gmax[2]) return false;
   const double fx = floor(tx), fy = floor(ty), fz = floor(tz);
   xl = int(fx);
   yl = int(fy);

@@ -168,7 +168,11 @@ __device__ __forceinline__ void combine_chunks_nf(const ShellLaunch &P, const Fr
 
 // Warp gw of shell launch P (32/C pixels, C lanes each) for the NF
 // frequency passes of Fq.  All 32 lanes of the warp call it with the same gw.
-template <int NG, bool kExt, int NF>
+// kFast: the launch's models are among B none/grid/spiral, n_e
+// none/grid/exponential disk and CRE_ana with a constant index (the host
+// checks, fast_models); the other models' paths are compiled out, so
+// the registers are allocated for this path alone.
+template <int NG, bool kExt, int NF, bool kFast = false>
 __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<NF> &Fq,
                                            long long gw, int lane) {
   const int C = P.chunks;
@@ -207,7 +211,7 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
     // |pos|^2 along the ray: |o|^2 + 2 (o.u) d + d^2
     const double ou2 = 2. * (ox * ux + oy * uy + oz * uz);
     const double oo = ox * ox + oy * oy + oz * oz;
-    const double r2min = P.gc_r_min * P.gc_r_min, r2max = P.gc_r_max * P.gc_r_max;
+    const double r2min = P.fast.r2min, r2max = P.fast.r2max;
     // Faraday phase in turns: rev0 + rev_k * (FD sum), per pass
     double rev0[NF], rev_k[NF];
     float a_s[NF];
@@ -219,10 +223,9 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
     }
     const DevModels &M = P.models;
     const FastModels &F = P.fast;
-    const float pe = float(P.em_pe);
+    const float pe = P.fast.pe;
     const bool pe2 = P.em_const && P.em_pe == 2.;
-    const float cre_ir0 = float(1. / M.cre_r0), cre_2iz0 = float(2. / M.cre_z0);
-    const float cre_R0 = float(M.cre_R0);
+    const float cre_ir0 = F.cre_ir0, cre_2iz0 = F.cre_2iz0, cre_R0 = F.cre_R0;
     // grid-space ray of group 0: g(d) = g0 + gv d
     double g0x = 0., g0y = 0., g0z = 0., gvx = 0., gvy = 0., gvz = 0.;
     if (NG == 1) {
@@ -237,7 +240,7 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
     // spiral B_par along the ray: amp/r * (K0 + K1 d)
     const double K0 = F.sp_sin * (ox * ux + oy * uy) + F.sp_cos * (ox * uy - oy * ux);
     const double K1 = F.sp_sin * (ux * ux + uy * uy);
-    const float spf = float(F.sp_sin), cpf = float(F.sp_cos);
+    const float spf = F.sp_sinf, cpf = F.sp_cosf;
     // I is one sum for all passes when the emissivity weight is frequency
     // independent (constant index); Q, U always one sum per pass
     constexpr int NI = NF;
@@ -247,10 +250,10 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
     bool i_shared = true;
     double sfd = 0., sdm = 0.;
     const bool fast_b = M.breg == kBregSpiral;
-    const bool slow_b = M.breg != kBregNone && M.breg != kBregGrid && !fast_b;
+    const bool slow_b = !kFast && M.breg != kBregNone && M.breg != kBregGrid && !fast_b;
     const bool fast_t = M.tereg == kTeregExpdisk;
-    const bool slow_t = M.tereg != kTeregNone && M.tereg != kTeregGrid && !fast_t;
-    const double rc2_hi = 400. * M.kpc * M.kpc, rc2_lo = 9. * M.kpc * M.kpc;
+    const bool slow_t = !kFast && M.tereg != kTeregNone && M.tereg != kTeregGrid && !fast_t;
+    const double rc2_hi = F.rc2_hi, rc2_lo = F.rc2_lo;
     float last_index = __int_as_float(0x7fc00000), gt = float(P.em_gt),
           gp = float(P.em_gp), inv1mi = 1.f;
     long long wlo, whi;
@@ -295,8 +298,8 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
       if (NG == 1) {
         const DevGridGroup &G = P.groups[0];
         const double gx = fma(gvx, d, g0x), gy = fma(gvy, d, g0y), gz = fma(gvz, d, g0z);
-        if (gx > 0. && gx < double(G.nx - 1) && gy > 0. && gy < double(G.ny - 1) &&
-            gz > 0. && gz < double(G.nz - 1)) {
+        if (gx > 0. && gx < G.gmax[0] && gy > 0. && gy < G.gmax[1] && gz > 0. &&
+            gz < G.gmax[2]) {
           int cx, cy, cz;
           float fx, fy, fz;
           cell_split(gx, G.nx - 2, cx, fx);
@@ -351,7 +354,7 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
           wps[0] = wp * ss2 * inv;
         } else {
           float prof;
-          if (M.cre == kCreAna) {
+          if (kFast || M.cre == kCreAna) {
             // exp((R0 - r)/r0) sech^2(z/z0)
             //   = 4 exp((R0 - r)/r0 - 2|z|/z0) / (1 + exp(-2|z|/z0))^2
             const float r2f = fmaf(xf, xf, yf * yf);
@@ -369,7 +372,7 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
             wps[0] = prof * ss2;
           } else {
             float wp[NF];
-            if (P.em_const) {
+            if (kFast || P.em_const) {
               const float bp = (pe == 1.f) ? sqrtf(rr) : powf(rr, 0.5f * pe);
               wt[0] = wp[0] = prof * bp;
             } else {
@@ -460,7 +463,7 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
 }
 
 // One frequency pass: the pass's constants from its launch block.
-template <int NG, bool kExt>
+template <int NG, bool kExt, bool kFast = false>
 __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw, int lane) {
   FreqSet<1> Fq;
   Fq.lambda2[0] = P.lambda2;
@@ -474,22 +477,22 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, long long gw, i
   Fq.out[0][0] = P.out[2];
   Fq.out[0][1] = P.out[3];
   Fq.out[0][2] = P.out[4];
-  fp32c_tile<NG, kExt, 1>(P, Fq, gw, lane);
+  fp32c_tile<NG, kExt, 1, kFast>(P, Fq, gw, lane);
 }
 
-template <int NG, bool kExt>
+template <int NG, bool kExt, bool kFast>
 __global__ void __launch_bounds__(256, HXG_FP32C_MIN_BLOCKS)
 shell_fp32c_kernel(const ShellLaunch P) {
-  fp32c_tile<NG, kExt>(P, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+  fp32c_tile<NG, kExt, kFast>(P, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
                        threadIdx.x & 31);
 }
 
 // NF frequency passes in one traversal of the shell (2 resident blocks: the
 // per-pass Q/U sums and phase constants take registers).
-template <int NG, bool kExt, int NF>
+template <int NG, bool kExt, int NF, bool kFast>
 __global__ void __launch_bounds__(HXG_FP32C_MULTI_THREADS, HXG_FP32C_MULTI_MIN_BLOCKS)
 shell_fp32c_multi_kernel(const ShellLaunch P, const FreqSet<NF> Fq) {
-  fp32c_tile<NG, kExt, NF>(P, Fq, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+  fp32c_tile<NG, kExt, NF, kFast>(P, Fq, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
                            threadIdx.x & 31);
 }
 

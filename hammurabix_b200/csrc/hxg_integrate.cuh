@@ -25,6 +25,13 @@ struct FastModels {
   double sp_b0, sp_irs, sp_crs, sp_ihs;  // amplitude, 1/r_s, r_sun/r_s, 1/h_s
   double sp_sin, sp_cos;                 // sin, cos of the pitch angle
   double ex_n0, ex_irn, ex_ihn;          // exp-disk n0, 1/r_s, 1/h_s
+  // launch constants in the types the sample loop uses, so that the loop
+  // reads them as operands instead of converting them
+  double r2min, r2max;                   // gc_r_min^2, gc_r_max^2
+  double rc2_hi, rc2_lo;                 // spiral cylinder: (20 kpc)^2, (3 kpc)^2
+  float sp_sinf, sp_cosf;                // sp_sin, sp_cos
+  float cre_ir0, cre_2iz0, cre_R0;       // CRE_ana: 1/r0, 2/z0, R0
+  float pe;                              // em_pe
 };
 
 // Everything one shell launch needs, in the working units of its form.
@@ -72,6 +79,19 @@ struct ShellLaunch {
   const ExtModels *ext;  // Jaffe / JF12 / YMW16 blocks (device), or null
 };
 
+// The models of the grid workloads: B none, grid or spiral; n_e none, grid
+// or exponential disk; CRE_ana with a constant index.  The shell kernels
+// have an instantiation (kFast) for launches whose models are among these,
+// with the other models' paths compiled out, so that its registers are
+// allocated for this path alone.
+__host__ __device__ inline bool fast_models(const ShellLaunch &P) {
+  const DevModels &M = P.models;
+  return P.ext == nullptr &&
+         (M.breg == kBregNone || M.breg == kBregGrid || M.breg == kBregSpiral) &&
+         (M.tereg == kTeregNone || M.tereg == kTeregGrid || M.tereg == kTeregExpdisk) &&
+         (!P.do_sync || (M.cre == kCreAna && P.em_const));
+}
+
 // The frequency-dependent constants of NF frequency passes that share one
 // shell traversal (same observer, shells, limits and models): each pass's
 // phase scale, emissivity scales, temp_convert and I/Q/U shell maps.  The
@@ -79,9 +99,10 @@ struct ShellLaunch {
 // depend on the frequency and are computed once for all NF passes.
 // Launch shape of the fused-frequency shell kernel: threads per block and
 // the resident blocks per SM its register budget is cut for.  128 x 5
-// (96 registers, a few spilled) keeps 20 warps per SM and ran config 3 in
-// 91.3 ms against 92.8 ms at 256 x 2 (128 registers) and 97.2 ms at
-// 128 x 6 (80 registers, more spills).
+// (96 registers) keeps 20 warps per SM; for the general instantiation it ran
+// config 3 in 91.3 ms against 92.8 ms at 256 x 2 (128 registers) and
+// 97.2 ms at 128 x 6 (80 registers, more spills); the kFast instantiation
+// needs no spill at 96 registers and is within 2 % at 128 x 4 and 128 x 6.
 #ifndef HXG_FP32C_MULTI_THREADS
 #define HXG_FP32C_MULTI_THREADS 128
 #endif
@@ -217,8 +238,9 @@ __device__ __forceinline__ void ipa2(T xv, T yv, T &c2, T &s2) {
 // FP64 parity form
 // ===================================================================
 // Warp gw of shell launch P (32/C pixels, C lanes each).  All 32 lanes of
-// the warp call it with the same gw.
-template <int NG, bool kCache, bool kExt>
+// the warp call it with the same gw.  kFast: the launch's models satisfy
+// fast_models (the same arithmetic, the other models compiled out).
+template <int NG, bool kCache, bool kExt, bool kFast = false>
 __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
                                           int lane) {
   const int C = P.chunks;
@@ -269,8 +291,15 @@ __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
           pz > P.gc_z_max)
         continue;
       const double p3[3] = {px, py, pz};
-      V3<double> B = breg_model_x<kExt>(M, P.ext, px, py, pz, p3);
-      double te = tereg_model_x<kExt>(M, P.ext, px, py, pz, p3);
+      V3<double> B{0., 0., 0.};
+      double te = 0.;
+      if (kFast) {
+        if (M.breg == kBregSpiral) B = breg_spiral<double>(M, px, py, pz, p3);
+        if (M.tereg == kTeregExpdisk) te = tereg_expdisk<double>(M, px, py, pz);
+      } else {
+        B = breg_model_x<kExt>(M, P.ext, px, py, pz, p3);
+        te = tereg_model_x<kExt>(M, P.ext, px, py, pz, p3);
+      }
       if (NG > 0) {
         double b3[3] = {B.x, B.y, B.z};
 #pragma unroll 1
@@ -298,7 +327,7 @@ __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
           jpol = jp * P.delta * P.i2bt;
         } else {
           double index = P.em_index;
-          if (!P.em_const) {
+          if (!kFast && !P.em_const) {
             index = cre_index<double>(M, px, py, pz);
             if (index != last_index) {
               gt = tgamma(-0.25 * index + 19. / 12.) * tgamma(-0.25 * index - 1. / 12.);
@@ -306,7 +335,8 @@ __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
               last_index = index;
             }
           }
-          const double fn = P.em_n0u * cre_profile<double>(M, px, py, pz, p3);
+          const double fn = P.em_n0u * (kFast ? cre_profile_ana<double>(M, px, py, pz)
+                                              : cre_profile<double>(M, px, py, pz, p3));
           const double absb = fabs(bper);
           const double A = P.em_anum / (P.em_3qe * absb);
           double Ae;
@@ -357,10 +387,10 @@ __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
   }
 }
 
-template <int NG, bool kCache, bool kExt>
+template <int NG, bool kCache, bool kExt, bool kFast = false>
 __global__ void __launch_bounds__(256)
 shell_fp64_kernel(const ShellLaunch P) {
-  fp64_tile<NG, kCache, kExt>(P, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+  fp64_tile<NG, kCache, kExt, kFast>(P, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
                               threadIdx.x & 31);
 }
 

@@ -57,13 +57,16 @@ cudaError_t launch_accumulate_transpose(cudaStream_t s, int nside_out,
                                         double *g_shell, double scale);
 cudaError_t launch_adjoint(cudaStream_t s, const AdjointLaunch &A,
                            unsigned blocks, unsigned threads);
-cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups, bool ext,
+// fast: every plan's models satisfy fast_models (the kFast instantiations).
+cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups, bool ext, bool fast,
                                const BatchLevel &B, unsigned blocks);
-cudaError_t batch_level_occupancy(bool fp32, int ngroups, bool ext, int *blocks_per_sm);
+cudaError_t batch_level_occupancy(bool fp32, int ngroups, bool ext, bool fast,
+                                  int *blocks_per_sm);
 // Fused-frequency plans (nf = 2 or 3): B points to a BatchLevelMulti<nf>.
-cudaError_t launch_batch_level_multi(cudaStream_t s, int ngroups, bool ext, int nf,
+cudaError_t launch_batch_level_multi(cudaStream_t s, int ngroups, bool ext, bool fast, int nf,
                                      const void *B, unsigned blocks);
-cudaError_t batch_multi_occupancy(int ngroups, bool ext, int nf, int *blocks_per_sm);
+cudaError_t batch_multi_occupancy(int ngroups, bool ext, bool fast, int nf,
+                                  int *blocks_per_sm);
 cudaError_t launch_batch_merge(cudaStream_t s, const MergeJob *jobs,
                                const unsigned long long *block0, int njobs,
                                unsigned long long nblocks);

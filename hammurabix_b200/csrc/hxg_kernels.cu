@@ -311,10 +311,16 @@ static cudaError_t by_shape(int ngroups, bool ext, F &&f) {
 
 cudaError_t launch_shell(cudaStream_t s, bool fp32, const ShellLaunch &P,
                          unsigned blocks, unsigned threads) {
+  const bool fast = fast_models(P);
   return by_shape(P.ngroups, P.ext != nullptr, [&](auto ng, auto ext) {
-    if (fp32)
-      shell_fp32c_kernel<decltype(ng)::value, decltype(ext)::value>
-          <<<blocks, threads, 0, s>>>(P);
+    constexpr int NG = decltype(ng)::value;
+    constexpr bool E = decltype(ext)::value;
+    if (fp32 && fast)
+      shell_fp32c_kernel<NG, false, true><<<blocks, threads, 0, s>>>(P);
+    else if (fp32)
+      shell_fp32c_kernel<NG, E, false><<<blocks, threads, 0, s>>>(P);
+    else if (fast)
+      shell_fp64_kernel<NG, false, false, true><<<blocks, threads, 0, s>>>(P);
     else
       shell_fp64_kernel<decltype(ng)::value, false, decltype(ext)::value>
           <<<blocks, threads, 0, s>>>(P);
@@ -323,62 +329,88 @@ cudaError_t launch_shell(cudaStream_t s, bool fp32, const ShellLaunch &P,
 
 cudaError_t launch_shell_multi(cudaStream_t s, const ShellLaunch &P, int nf, const void *fq,
                                unsigned blocks, unsigned threads) {
+  const bool fast = fast_models(P);
   return by_shape(P.ngroups, P.ext != nullptr, [&](auto ng, auto ext) {
     constexpr int NG = decltype(ng)::value;
     constexpr bool E = decltype(ext)::value;
-    if (nf == 2)
-      shell_fp32c_multi_kernel<NG, E, 2>
-          <<<blocks, threads, 0, s>>>(P, *static_cast<const FreqSet<2> *>(fq));
+    const FreqSet<2> &F2 = *static_cast<const FreqSet<2> *>(fq);
+    const FreqSet<3> &F3 = *static_cast<const FreqSet<3> *>(fq);
+    if (fast && nf == 2)
+      shell_fp32c_multi_kernel<NG, false, 2, true><<<blocks, threads, 0, s>>>(P, F2);
+    else if (fast)
+      shell_fp32c_multi_kernel<NG, false, 3, true><<<blocks, threads, 0, s>>>(P, F3);
+    else if (nf == 2)
+      shell_fp32c_multi_kernel<NG, E, 2, false><<<blocks, threads, 0, s>>>(P, F2);
     else
-      shell_fp32c_multi_kernel<NG, E, 3>
-          <<<blocks, threads, 0, s>>>(P, *static_cast<const FreqSet<3> *>(fq));
+      shell_fp32c_multi_kernel<NG, E, 3, false><<<blocks, threads, 0, s>>>(P, F3);
   });
 }
 
-cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups, bool ext,
+cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups, bool ext, bool fast,
                                const BatchLevel &B, unsigned blocks) {
   return by_shape(ngroups, ext, [&](auto ng, auto ex) {
-    if (fp32)
-      batch_fp32c_kernel<decltype(ng)::value, decltype(ex)::value><<<blocks, 256, 0, s>>>(B);
+    constexpr int NG = decltype(ng)::value;
+    constexpr bool E = decltype(ex)::value;
+    if (fp32 && fast)
+      batch_fp32c_kernel<NG, false, true><<<blocks, 256, 0, s>>>(B);
+    else if (fp32)
+      batch_fp32c_kernel<NG, E, false><<<blocks, 256, 0, s>>>(B);
+    else if (fast)
+      batch_fp64_kernel<NG, false, true><<<blocks, 256, 0, s>>>(B);
     else
-      batch_fp64_kernel<decltype(ng)::value, decltype(ex)::value><<<blocks, 256, 0, s>>>(B);
+      batch_fp64_kernel<NG, E, false><<<blocks, 256, 0, s>>>(B);
   });
 }
 
-cudaError_t launch_batch_level_multi(cudaStream_t s, int ngroups, bool ext, int nf,
+cudaError_t launch_batch_level_multi(cudaStream_t s, int ngroups, bool ext, bool fast, int nf,
                                      const void *B, unsigned blocks) {
   return by_shape(ngroups, ext, [&](auto ng, auto ex) {
     constexpr int NG = decltype(ng)::value;
     constexpr bool E = decltype(ex)::value;
-    if (nf == 2)
-      batch_fp32c_multi_kernel<NG, E, 2>
-          <<<blocks, 256, 0, s>>>(*static_cast<const BatchLevelMulti<2> *>(B));
+    const auto &B2 = *static_cast<const BatchLevelMulti<2> *>(B);
+    const auto &B3 = *static_cast<const BatchLevelMulti<3> *>(B);
+    if (fast && nf == 2)
+      batch_fp32c_multi_kernel<NG, false, 2, true><<<blocks, 256, 0, s>>>(B2);
+    else if (fast)
+      batch_fp32c_multi_kernel<NG, false, 3, true><<<blocks, 256, 0, s>>>(B3);
+    else if (nf == 2)
+      batch_fp32c_multi_kernel<NG, E, 2, false><<<blocks, 256, 0, s>>>(B2);
     else
-      batch_fp32c_multi_kernel<NG, E, 3>
-          <<<blocks, 256, 0, s>>>(*static_cast<const BatchLevelMulti<3> *>(B));
+      batch_fp32c_multi_kernel<NG, E, 3, false><<<blocks, 256, 0, s>>>(B3);
   });
 }
 
-cudaError_t batch_multi_occupancy(int ngroups, bool ext, int nf, int *blocks_per_sm) {
+cudaError_t batch_multi_occupancy(int ngroups, bool ext, bool fast, int nf, int *blocks_per_sm) {
   const void *f = nullptr;
   by_shape(ngroups, ext, [&](auto ng, auto ex) {
     constexpr int NG = decltype(ng)::value;
     constexpr bool E = decltype(ex)::value;
-    if (nf == 2)
-      f = (const void *)batch_fp32c_multi_kernel<NG, E, 2>;
+    if (fast && nf == 2)
+      f = (const void *)batch_fp32c_multi_kernel<NG, false, 2, true>;
+    else if (fast)
+      f = (const void *)batch_fp32c_multi_kernel<NG, false, 3, true>;
+    else if (nf == 2)
+      f = (const void *)batch_fp32c_multi_kernel<NG, E, 2, false>;
     else
-      f = (const void *)batch_fp32c_multi_kernel<NG, E, 3>;
+      f = (const void *)batch_fp32c_multi_kernel<NG, E, 3, false>;
   });
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, 256, 0);
 }
 
-cudaError_t batch_level_occupancy(bool fp32, int ngroups, bool ext, int *blocks_per_sm) {
+cudaError_t batch_level_occupancy(bool fp32, int ngroups, bool ext, bool fast,
+                                  int *blocks_per_sm) {
   const void *f = nullptr;
   by_shape(ngroups, ext, [&](auto ng, auto ex) {
-    if (fp32)
-      f = (const void *)batch_fp32c_kernel<decltype(ng)::value, decltype(ex)::value>;
+    constexpr int NG = decltype(ng)::value;
+    constexpr bool E = decltype(ex)::value;
+    if (fp32 && fast)
+      f = (const void *)batch_fp32c_kernel<NG, false, true>;
+    else if (fp32)
+      f = (const void *)batch_fp32c_kernel<NG, E, false>;
+    else if (fast)
+      f = (const void *)batch_fp64_kernel<NG, false, true>;
     else
-      f = (const void *)batch_fp64_kernel<decltype(ng)::value, decltype(ex)::value>;
+      f = (const void *)batch_fp64_kernel<NG, E, false>;
   });
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, 256, 0);
 }
