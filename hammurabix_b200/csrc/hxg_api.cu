@@ -1342,7 +1342,7 @@ int run_shell(hxg_handle *h, const hxg_obs_t &o, uint32_t s, const ExtModels *ex
   }
   if (local == 0) return HXG_OK;
   const uint64_t warps = (local + (32 / C) - 1) / (32 / C);
-  const unsigned threads = 256;
+  const unsigned threads = fp32 ? HXG_FP32C_THREADS : 256;
   const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (h->timing) {
