@@ -16,7 +16,8 @@
 //   - the phase, reduced to a fraction of a turn with integer operations.
 // FP32 carries the trilinear grid interpolation (FP32 voxel records, whose
 // rounding is random from sample to sample), the synchrotron emissivity and
-// polarisation angle, and Kahan-compensated I, Q, U sums.
+// polarisation angle, and the I, Q, U sums (FP32 over blocks of 16 samples,
+// Kahan-compensated across blocks).
 //
 // Speed.  The kernel is issue/latency bound (the grids stay in L1/L2) with
 // the XU pipe (MUFU and conversions) the busiest: the cell index and
@@ -252,9 +253,9 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
     // I is one sum for all passes when the emissivity weight is frequency
     // independent (constant index); Q, U always one sum per pass
     constexpr int NI = NF;
-    KahanF ki[NI], kq[NF], ku[NF];
+    BlockKahanF ki[NI], kq[NF], ku[NF];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) ki[f] = kq[f] = ku[f] = KahanF{0.f, 0.f};
+    for (int f = 0; f < NF; ++f) ki[f] = kq[f] = ku[f] = BlockKahanF{0.f, KahanF{0.f, 0.f}};
     bool i_shared = true;
     double sfd = 0., sdm = 0.;
     const bool fast_b = M.breg == kBregSpiral;
@@ -270,6 +271,14 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
     const long long i1 = min((P.step * (c + 1)) >> P.log2_chunks, whi);
     double d = P.d_start + ((double)i0 + 0.5) * P.delta;
     for (long long i = i0; i < i1; ++i, d += P.delta) {
+      if ((i & 15) == 0) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+          if (f == 0 || !i_shared) ki[f].flush();
+          kq[f].flush();
+          ku[f].flush();
+        }
+      }
       const double pz = fma(uz, d, oz);
       const double r2 = fma(d, d + ou2, oo);
       if (r2 < r2min || r2 > r2max || pz < P.gc_z_min || pz > P.gc_z_max) continue;

@@ -180,6 +180,25 @@ struct KahanF {
   }
 };
 
+// Two-level FP32 sum: a plain running sum over a block of samples, folded
+// into a Kahan-compensated total by flush() (the caller flushes every 16
+// sample indices).  The block sums' rounding (a few ulp of at most 16
+// terms) is random from block to block, and the total is compensated.
+struct BlockKahanF {
+  float acc;
+  KahanF tot;
+  __device__ __forceinline__ void add(float v) { acc += v; }
+  __device__ __forceinline__ void flush() {
+    tot.add(acc);
+    acc = 0.f;
+  }
+  __device__ __forceinline__ double value() const {
+    KahanF t = tot;
+    t.add(acc);
+    return t.value();
+  }
+};
+
 __device__ __forceinline__ double shfl_xor_d(double v, int o) {
   return __shfl_xor_sync(0xffffffffu, v, o);
 }
