@@ -64,8 +64,22 @@ __device__ __forceinline__ void flush_cell(double *grad_rec, long long key,
       }
 }
 
-template <int NG, bool kExt>
-__global__ void __launch_bounds__(256)
+// Launch shape of the adjoint shell kernel (threads per block, resident
+// blocks per SM its register allocation must allow).  128 x 3 (168
+// registers, 12 warps per SM; the per-cell gradient accumulators take 64)
+// ran the config-4 adjoint in 49.9 ms against 52.4 ms at 128 x 4 (128
+// registers, more spills) and 62.2 ms at 256 x 1 (254 registers, 8 warps).
+#ifndef HXG_ADJ_THREADS
+#define HXG_ADJ_THREADS 128
+#endif
+#ifndef HXG_ADJ_MIN_BLOCKS
+#define HXG_ADJ_MIN_BLOCKS 3
+#endif
+
+// kFast: the forward launch's models satisfy fast_models (the other models
+// compiled out).
+template <int NG, bool kExt, bool kFast>
+__global__ void __launch_bounds__(HXG_ADJ_THREADS, HXG_ADJ_MIN_BLOCKS)
 shell_fp64_adjoint_kernel(const AdjointLaunch A) {
   const ShellLaunch &P = A.F;
   const int lane = threadIdx.x & 31;
@@ -177,8 +191,15 @@ shell_fp64_adjoint_kernel(const AdjointLaunch A) {
           pz > P.gc_z_max)
         continue;
       const double p3[3] = {px, py, pz};
-      const V3<double> Breg = breg_model_x<kExt>(M, P.ext, px, py, pz, p3);
-      const double tereg = tereg_model_x<kExt>(M, P.ext, px, py, pz, p3);
+      V3<double> Breg{0., 0., 0.};
+      double tereg = 0.;
+      if (kFast) {
+        if (M.breg == kBregSpiral) Breg = breg_spiral<double>(M, px, py, pz, p3);
+        if (M.tereg == kTeregExpdisk) tereg = tereg_expdisk<double>(M, px, py, pz);
+      } else {
+        Breg = breg_model_x<kExt>(M, P.ext, px, py, pz, p3);
+        tereg = tereg_model_x<kExt>(M, P.ext, px, py, pz, p3);
+      }
       double b3[3] = {Breg.x, Breg.y, Breg.z};
       double te = tereg;
       bool in_grid = false;
@@ -215,7 +236,7 @@ shell_fp64_adjoint_kernel(const AdjointLaunch A) {
         double gtt = gfd;
         if (P.do_sync) {
           double index = P.em_index;
-          if (!P.em_const) {
+          if (!kFast && !P.em_const) {
             index = cre_index<double>(M, px, py, pz);
             if (index != last_index) {
               gt = tgamma(-0.25 * index + 19. / 12.) * tgamma(-0.25 * index - 1. / 12.);
@@ -224,7 +245,8 @@ shell_fp64_adjoint_kernel(const AdjointLaunch A) {
             }
           }
           e = 0.5 * (index + 1);
-          const double fn = P.em_n0u * cre_profile<double>(M, px, py, pz, p3);
+          const double fn = P.em_n0u * (kFast ? cre_profile_ana<double>(M, px, py, pz)
+                                              : cre_profile<double>(M, px, py, pz, p3));
           const double absb = fabs(bper);
           const double Aa = P.em_anum / (P.em_3qe * absb);
           double Ae;

@@ -1342,7 +1342,7 @@ int run_shell(hxg_handle *h, const hxg_obs_t &o, uint32_t s, const ExtModels *ex
   }
   if (local == 0) return HXG_OK;
   const uint64_t warps = (local + (32 / C) - 1) / (32 / C);
-  const unsigned threads = fp32 ? HXG_FP32C_THREADS : 256;
+  const unsigned threads = fp32 ? HXG_FP32C_THREADS : HXG_FP64_THREADS;
   const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (h->timing) {
@@ -1871,7 +1871,7 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
     A.g_fdmap = gfdmap;
     A.want_j0 = (h->models.cre == HXG_CRE_ANA || h->models.cre == HXG_CRE_UNIF) ? 1 : 0;
     const uint64_t warps = (npix + (32 / C) - 1) / (32 / C);
-    const unsigned threads = 256;
+    const unsigned threads = HXG_ADJ_THREADS;
     const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
     HXG_CK(launch_adjoint(h->stream, A, blocks, threads));
     ++h->launch_count;

@@ -71,9 +71,19 @@ __device__ __forceinline__ void batch_multi_body(const BatchLevelMulti<NF> &B) {
   }
 }
 
+// Launch shape of the fused batch kernel (threads per block, resident
+// blocks per SM its register allocation must allow).  256 x 2 ran config 5
+// in 1149 ms against 1214-1216 ms at 128 x 5 and 128 x 6.
+#ifndef HXG_BATCH_MULTI_THREADS
+#define HXG_BATCH_MULTI_THREADS 256
+#endif
+#ifndef HXG_BATCH_MULTI_MIN_BLOCKS
+#define HXG_BATCH_MULTI_MIN_BLOCKS 2
+#endif
+
 // kFast: every plan's models satisfy fast_models.
 template <int NG, bool kExt, int NF, bool kFast>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(HXG_BATCH_MULTI_THREADS, HXG_BATCH_MULTI_MIN_BLOCKS)
 batch_fp32c_multi_kernel(const BatchLevelMulti<NF> B) {
   batch_multi_body<NG, kExt, NF, kFast>(B);
 }

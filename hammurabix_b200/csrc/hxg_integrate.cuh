@@ -406,8 +406,21 @@ __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
   }
 }
 
+// Launch shape of the FP64 shell kernel: threads per block and the resident
+// blocks per SM its register allocation must allow.  128 x 7 (72
+// registers, 28 warps per SM) ran the config-3 FP64 passes in 490.6 ms
+// against 492.7 ms at 128 x 6, 494.0 ms at 256 x 3, 499.5 ms at 256 x 4,
+// 513 ms at 128 x 5, 566 ms at 128 x 4 and 574 ms with the compiler's own
+// choice at 256 threads (104 registers, 16 warps).
+#ifndef HXG_FP64_THREADS
+#define HXG_FP64_THREADS 128
+#endif
+#ifndef HXG_FP64_MIN_BLOCKS
+#define HXG_FP64_MIN_BLOCKS 7
+#endif
+
 template <int NG, bool kCache, bool kExt, bool kFast = false>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(HXG_FP64_THREADS, HXG_FP64_MIN_BLOCKS)
 shell_fp64_kernel(const ShellLaunch P) {
   fp64_tile<NG, kCache, kExt, kFast>(P, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
                               threadIdx.x & 31);

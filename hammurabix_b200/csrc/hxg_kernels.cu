@@ -370,13 +370,13 @@ cudaError_t launch_batch_level_multi(cudaStream_t s, int ngroups, bool ext, bool
     const auto &B2 = *static_cast<const BatchLevelMulti<2> *>(B);
     const auto &B3 = *static_cast<const BatchLevelMulti<3> *>(B);
     if (fast && nf == 2)
-      batch_fp32c_multi_kernel<NG, false, 2, true><<<blocks, 256, 0, s>>>(B2);
+      batch_fp32c_multi_kernel<NG, false, 2, true><<<blocks, HXG_BATCH_MULTI_THREADS, 0, s>>>(B2);
     else if (fast)
-      batch_fp32c_multi_kernel<NG, false, 3, true><<<blocks, 256, 0, s>>>(B3);
+      batch_fp32c_multi_kernel<NG, false, 3, true><<<blocks, HXG_BATCH_MULTI_THREADS, 0, s>>>(B3);
     else if (nf == 2)
-      batch_fp32c_multi_kernel<NG, E, 2, false><<<blocks, 256, 0, s>>>(B2);
+      batch_fp32c_multi_kernel<NG, E, 2, false><<<blocks, HXG_BATCH_MULTI_THREADS, 0, s>>>(B2);
     else
-      batch_fp32c_multi_kernel<NG, E, 3, false><<<blocks, 256, 0, s>>>(B3);
+      batch_fp32c_multi_kernel<NG, E, 3, false><<<blocks, HXG_BATCH_MULTI_THREADS, 0, s>>>(B3);
   });
 }
 
@@ -394,7 +394,7 @@ cudaError_t batch_multi_occupancy(int ngroups, bool ext, bool fast, int nf, int 
     else
       f = (const void *)batch_fp32c_multi_kernel<NG, E, 3, false>;
   });
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, 256, 0);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, HXG_BATCH_MULTI_THREADS, 0);
 }
 
 cudaError_t batch_level_occupancy(bool fp32, int ngroups, bool ext, bool fast,
@@ -479,12 +479,22 @@ cudaError_t launch_accumulate_transpose(cudaStream_t s, int nside_out,
 cudaError_t launch_adjoint(cudaStream_t s, const AdjointLaunch &A,
                            unsigned blocks, unsigned threads) {
   const bool ext = A.F.ext != nullptr;
-  if (A.F.ngroups == 0)
-    ext ? shell_fp64_adjoint_kernel<0, true><<<blocks, threads, 0, s>>>(A)
-        : shell_fp64_adjoint_kernel<0, false><<<blocks, threads, 0, s>>>(A);
-  else
-    ext ? shell_fp64_adjoint_kernel<1, true><<<blocks, threads, 0, s>>>(A)
-        : shell_fp64_adjoint_kernel<1, false><<<blocks, threads, 0, s>>>(A);
+  const bool fast = fast_models(A.F);
+  if (A.F.ngroups == 0) {
+    if (fast)
+      shell_fp64_adjoint_kernel<0, false, true><<<blocks, threads, 0, s>>>(A);
+    else if (ext)
+      shell_fp64_adjoint_kernel<0, true, false><<<blocks, threads, 0, s>>>(A);
+    else
+      shell_fp64_adjoint_kernel<0, false, false><<<blocks, threads, 0, s>>>(A);
+  } else {
+    if (fast)
+      shell_fp64_adjoint_kernel<1, false, true><<<blocks, threads, 0, s>>>(A);
+    else if (ext)
+      shell_fp64_adjoint_kernel<1, true, false><<<blocks, threads, 0, s>>>(A);
+    else
+      shell_fp64_adjoint_kernel<1, false, false><<<blocks, threads, 0, s>>>(A);
+  }
   return cudaGetLastError();
 }
 

@@ -121,7 +121,7 @@ extern "C" int hxg_write_grid_noalloc(const hxg_obs_t *obs,
     // whole warps of 32 pixels, one lane per pixel
     P.chunks = 1;
     P.log2_chunks = 0;
-    const unsigned threads = 256;
+    const unsigned threads = HXG_FP64_THREADS;
     const unsigned blocks = (unsigned)((npix + threads - 1) / threads);
     if (launch_shell(s, false, P, blocks, threads) != cudaSuccess) return HXG_ERR_CUDA;
     const int ns = (int)obs->nside_shell[sh];
