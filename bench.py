@@ -568,12 +568,14 @@ def main():
             # one handle, one stream, steps one after another
             e2e_streams = [stream]
         else:
-            # two handles on two streams: step k+1's grids cross PCIe (the
-            # upload returns when its copies are done) while step k runs on
-            # the other stream, and step k's maps come back while step k+1
-            # runs; every step still uploads its own grids and reads back
-            # its own maps inside the timed region
+            # two handles on two streams and a read-back stream: step k+1's
+            # grids cross PCIe (the upload returns when its copies are done)
+            # while step k computes, and step k's maps come back (the other
+            # direction) while step k+1 computes; every step still uploads
+            # its own grids and reads back its own maps inside the timed
+            # region
             e2e_streams = [stream, torch.cuda.Stream(dev)]
+        rb_stream = torch.cuda.Stream(dev)
         iges = [e2e_integ(s) for s in e2e_streams]
         e2e_outs = [outputs() for _ in iges]
         pinned_outs = [[{k: torch.empty(npx, dtype=torch.float64, pin_memory=True).numpy()
@@ -581,17 +583,36 @@ def main():
 
         def e2e_run(nsteps):
             npipe = len(iges)
+            comp = [None] * npipe   # per handle: its last step's compute is done
+            home = [None] * npipe   # per handle: its last step's maps are home
             upload(iges[0])
             for k in range(nsteps):
                 a, b = k % npipe, (k + 1) % npipe
-                with torch.cuda.stream(e2e_streams[a]):
+                sa = e2e_streams[a]
+                if npipe == 1:
+                    with torch.cuda.stream(sa):
+                        step(iges[a], e2e_outs[a])
+                        read_back(e2e_outs[a], pinned_outs[a])
+                    sa.synchronize()
+                    if k + 1 < nsteps:
+                        upload(iges[a])
+                    continue
+                with torch.cuda.stream(sa):
+                    if home[a] is not None:
+                        sa.wait_event(home[a])   # step k-2's maps have left the outputs
                     step(iges[a], e2e_outs[a])
+                    comp[a] = torch.cuda.Event()
+                    comp[a].record(sa)
+                rb_stream.wait_event(comp[a])
+                with torch.cuda.stream(rb_stream):
                     read_back(e2e_outs[a], pinned_outs[a])
+                    home[a] = torch.cuda.Event()
+                    home[a].record(rb_stream)
                 if k + 1 < nsteps:
-                    e2e_streams[b].synchronize()    # step k-1 (or k) done, maps home
+                    if comp[b] is not None:
+                        comp[b].synchronize()    # step k-1 no longer reads b's grids
                     upload(iges[b])
-            for s in e2e_streams:
-                s.synchronize()
+            torch.cuda.synchronize(dev)
 
         e2e_run(2)
         barrier()
@@ -605,8 +626,9 @@ def main():
         e2e = {"value": (1 if shard else ws) * samples_step / te, "unit": UNIT,
                "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": te * 1e3,
-               "overlap": ("two handles on two streams: step k+1's upload and step k-1's "
-                           "read-back overlap step k") if len(iges) > 1 else "none"}
+               "overlap": ("two handles on two streams and a read-back stream: step k+1's "
+                           "upload and step k-1's read-back overlap step k") if len(iges) > 1
+               else "none"}
         for ig_ in iges:
             ig_.close()
         del pinned, hosts, pinned_outs
