@@ -504,8 +504,9 @@ shell_fp32c_kernel(const ShellLaunch P) {
                        threadIdx.x & 31);
 }
 
-// NF frequency passes in one traversal of the shell (2 resident blocks: the
-// per-pass Q/U sums and phase constants take registers).
+// NF frequency passes in one traversal of the shell (launch shape
+// HXG_FP32C_MULTI_THREADS x HXG_FP32C_MULTI_MIN_BLOCKS: the per-pass Q/U
+// sums and phase constants take registers).
 template <int NG, bool kExt, int NF, bool kFast>
 __global__ void __launch_bounds__(HXG_FP32C_MULTI_THREADS, HXG_FP32C_MULTI_MIN_BLOCKS)
 shell_fp32c_multi_kernel(const ShellLaunch P, const FreqSet<NF> Fq) {
