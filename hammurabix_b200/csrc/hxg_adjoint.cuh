@@ -177,8 +177,8 @@ shell_fp64_adjoint_kernel(const AdjointLaunch A) {
     long long acc_key = -1;
     double gt = P.em_gt, gpp = P.em_gp, last_index = nan("");
     double fdl = 0.;  // running FD of this chunk
-    long long wlo, whi;
-    ray_window(P, ux, uy, uz, wlo, whi);
+    long long wlo, whi, slo_unused, shi_unused;
+    ray_window(P, ux, uy, uz, wlo, whi, slo_unused, shi_unused);
     const long long i0 = max((P.step * c) >> P.log2_chunks, wlo);
     const long long i1 = min((P.step * (c + 1)) >> P.log2_chunks, whi);
     for (long long i = i0; i < i1; ++i) {
@@ -186,6 +186,7 @@ shell_fp64_adjoint_kernel(const AdjointLaunch A) {
       const double px = ux * d + P.obs[0];
       const double py = uy * d + P.obs[1];
       const double pz = uz * d + P.obs[2];
+      // every sample is tested (the certain window measured slower here)
       const double len = sqrt(px * px + py * py + pz * pz);
       if (len < P.gc_r_min || len > P.gc_r_max || pz < P.gc_z_min ||
           pz > P.gc_z_max)

@@ -265,8 +265,8 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
     const double rc2_hi = F.rc2_hi, rc2_lo = F.rc2_lo;
     float last_index = __int_as_float(0x7fc00000), gt = float(P.em_gt),
           gp = float(P.em_gp), inv1mi = 1.f;
-    long long wlo, whi;
-    ray_window(P, ux, uy, uz, wlo, whi);
+    long long wlo, whi, slo_unused, shi_unused;
+    ray_window(P, ux, uy, uz, wlo, whi, slo_unused, shi_unused);
     const long long i0 = max((P.step * c) >> P.log2_chunks, wlo);
     const long long i1 = min((P.step * (c + 1)) >> P.log2_chunks, whi);
     double d = P.d_start + ((double)i0 + 0.5) * P.delta;
@@ -279,6 +279,8 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
           ku[f].flush();
         }
       }
+      // every sample is tested: the test costs less here than the two
+      // extra live window bounds (measured)
       const double pz = fma(uz, d, oz);
       const double r2 = fma(d, d + ou2, oo);
       if (r2 < r2min || r2 > r2max || pz < P.gc_z_min || pz > P.gc_z_max) continue;

@@ -134,17 +134,21 @@ __device__ __forceinline__ unsigned long long shard_nest(const ShellLaunch &P,
 // spherical |pos| <= r_max and vertical z_min <= z <= z_max cuts
 // (integrator.cc:179-182), from the roots of |o + u d|^2 = r_max^2 and
 // o_z + u_z d = z_min / z_max, widened by two samples on each side.  Samples
-// outside the window fail the cuts; every sample inside is still tested
-// exactly, so the window only saves the iterations that would be skipped.
+// outside the window fail the cuts; the samples of [slo, shi) lie two or
+// more steps inside it and pass them for certain, the others inside the
+// window are tested exactly, so the result is the per-sample test's.
 __device__ __forceinline__ void ray_window(const ShellLaunch &P, double ux,
                                            double uy, double uz,
-                                           long long &lo, long long &hi) {
+                                           long long &lo, long long &hi,
+                                           long long &slo, long long &shi) {
   const double ox = P.obs[0], oy = P.obs[1], oz = P.obs[2];
   const double b = ox * ux + oy * uy + oz * uz;  // o.u
   const double c = (ox * ox + oy * oy + oz * oz) - P.gc_r_max * P.gc_r_max;
   const double disc = b * b - c;
   lo = 0;
   hi = 0;
+  slo = 0;
+  shi = 0;
   if (!(disc >= 0.)) return;  // the ray misses the r_max sphere
   const double sq = sqrt(disc);
   double da = -b - sq, db = -b + sq;
@@ -160,10 +164,19 @@ __device__ __forceinline__ void ray_window(const ShellLaunch &P, double ux,
   if (!(da <= db)) return;
   // d_i = d_start + (i + 1/2) delta
   const double n = (double)P.step;
-  const double fa = fmin(fmax(floor((da - P.d_start) / P.delta - 0.5) - 2., 0.), n);
-  const double fb = fmin(fmax(ceil((db - P.d_start) / P.delta - 0.5) + 3., 0.), n);
+  const double xa = (da - P.d_start) / P.delta - 0.5, xb = (db - P.d_start) / P.delta - 0.5;
+  const double fa = fmin(fmax(floor(xa) - 2., 0.), n);
+  const double fb = fmin(fmax(ceil(xb) + 3., 0.), n);
   lo = (long long)fa;
   hi = (long long)fb;
+  // samples two or more steps inside both ends pass the cuts for certain
+  // (the rounding of da, db and of the sample positions is ~1e-12 of a
+  // step); with an inner radius the ray may cross the r_min ball, so every
+  // sample is tested
+  if (!(P.gc_r_min > 0.)) {
+    slo = (long long)fmin(fmax(ceil(xa) + 2., 0.), n);
+    shi = (long long)fmin(fmax(floor(xb) - 1., 0.), n);
+  }
 }
 
 // Kahan-compensated FP32 accumulator.
@@ -296,8 +309,8 @@ __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
     CellCache<double> cache;
     cache.key = -1;
     double last_index = nan(""), gt = P.em_gt, gp = P.em_gp;
-    long long wlo, whi;
-    ray_window(P, ux, uy, uz, wlo, whi);
+    long long wlo, whi, slo, shi;
+    ray_window(P, ux, uy, uz, wlo, whi, slo, shi);
     const long long i0 = max((P.step * c) >> P.log2_chunks, wlo);
     const long long i1 = min((P.step * (c + 1)) >> P.log2_chunks, whi);
     for (long long i = i0; i < i1; ++i) {
@@ -305,10 +318,12 @@ __device__ __forceinline__ void fp64_tile(const ShellLaunch &P, long long gw,
       const double px = ux * d + P.obs[0];
       const double py = uy * d + P.obs[1];
       const double pz = uz * d + P.obs[2];
-      const double len = sqrt(px * px + py * py + pz * pz);
-      if (len < P.gc_r_min || len > P.gc_r_max || pz < P.gc_z_min ||
-          pz > P.gc_z_max)
-        continue;
+      if (i < slo || i >= shi) {
+        const double len = sqrt(px * px + py * py + pz * pz);
+        if (len < P.gc_r_min || len > P.gc_r_max || pz < P.gc_z_min ||
+            pz > P.gc_z_max)
+          continue;
+      }
       const double p3[3] = {px, py, pz};
       V3<double> B{0., 0., 0.};
       double te = 0.;
