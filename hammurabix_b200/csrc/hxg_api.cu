@@ -151,6 +151,10 @@ bool models_supported(const hxg_models_t &m, std::string *why) {
       *why = "regular B model not supported on the device";
       return false;
   }
+  if (m.breg == HXG_BREG_JAFFE && m.jaffe.arm_num > 8) {
+    *why = "Breg_jaffe with more than 8 spiral arms";
+    return false;
+  }
   if (m.brnd != HXG_BRND_NONE && m.brnd != HXG_BRND_GRID) {
     *why = "random B model must be NONE or GRID";
     return false;

@@ -10,7 +10,8 @@
 // The array is a file-scope __device__ variable: every GPU that loads this
 // library holds it until the process exits.  Host code never uses its name
 // as an address (in host code the name is only a stand-in symbol); the
-// device address is looked up once per device with cudaGetSymbolAddress.
+// device address is looked up with cudaGetSymbolAddress once per CUDA
+// context, with that context current.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -35,25 +36,78 @@ constexpr uint64_t kMaxShellPix = 12ull * HXG_NOALLOC_MAX_NSIDE * HXG_NOALLOC_MA
 // Five shell maps (dm, fd, I, Q, U) at the largest allowed shell Nside.
 static __device__ __align__(256) double g_noalloc_scratch[5 * kMaxShellPix];
 
-constexpr int kMaxDevices = 64;
-std::once_flag g_once[kMaxDevices];
-double *g_scratch_ptr[kMaxDevices] = {};
-cudaError_t g_setup_err[kMaxDevices] = {};
+// Device addresses of the scratch array, one per CUDA context that has
+// called in.  A context is named by its driver-assigned ID (cuCtxGetId),
+// which is never reused within the process: after cudaDeviceReset the
+// module is loaded again into a new context, the array may move, and the
+// new context's ID misses this table, so the address is looked up again.
+// Only successful lookups are stored; a failed one is retried next call.
+struct ScratchEntry {
+  unsigned long long ctx_id;
+  double *ptr;
+};
+constexpr int kMaxContexts = 64;
+std::mutex g_mu;
+ScratchEntry g_entries[kMaxContexts] = {};
+int g_next_entry = 0;  // slot reused next when the table is full
 
-// Device address of the scratch array on the current device; looked up on
-// the first call on each device, with that device current.
-int scratch_for_current_device(double **out) {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess) return HXG_ERR_NO_DEVICE;
-  if (dev < 0 || dev >= kMaxDevices) return HXG_ERR_UNSUPPORTED;
-  std::call_once(g_once[dev], [dev]() {
-    void *p = nullptr;
-    g_setup_err[dev] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    g_scratch_ptr[dev] = static_cast<double *>(p);
+using CtxGetCurrentFn = int (*)(void **ctx);
+using CtxGetIdFn = int (*)(void *ctx, unsigned long long *id);
+
+// ID of the context current on this thread; 0 when there is none yet.
+// The driver functions are fetched through the runtime, so the library
+// needs no link-time libcuda.
+bool current_context_id(unsigned long long *id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, []() {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault,
+                                         &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
   });
-  if (g_setup_err[dev] != cudaSuccess || g_scratch_ptr[dev] == nullptr)
+  if (get_current == nullptr || get_id == nullptr) return false;
+  void *ctx = nullptr;
+  if (get_current(&ctx) != 0) return false;
+  if (ctx == nullptr) {
+    *id = 0;
+    return true;
+  }
+  return get_id(ctx, id) == 0;
+}
+
+// Device address of the scratch array in the current context (the
+// current device's primary context for runtime-API callers).  The first
+// call in a context looks it up with cudaGetSymbolAddress, which also
+// creates the primary context when none is current yet.
+int scratch_for_current_context(double **out) {
+  unsigned long long id = 0;
+  if (!current_context_id(&id)) return HXG_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (id != 0)
+    for (const ScratchEntry &e : g_entries)
+      if (e.ctx_id == id && e.ptr != nullptr) {
+        *out = e.ptr;
+        return HXG_OK;
+      }
+  void *p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) {
+    (void)cudaGetLastError();  // the failure is reported by the status
     return HXG_ERR_CUDA;
-  *out = g_scratch_ptr[dev];
+  }
+  // the lookup made a context current if none was
+  if (id == 0 && (!current_context_id(&id) || id == 0)) return HXG_ERR_CUDA;
+  g_entries[g_next_entry] = ScratchEntry{id, static_cast<double *>(p)};
+  g_next_entry = (g_next_entry + 1) % kMaxContexts;
+  *out = static_cast<double *>(p);
   return HXG_OK;
 }
 
@@ -87,8 +141,11 @@ extern "C" int hxg_write_grid_noalloc(const hxg_obs_t *obs,
     return HXG_ERR_INVALID;
   for (uint32_t s = 0; s < obs->total_shell; ++s)
     if (obs->nside_shell[s] > HXG_NOALLOC_MAX_NSIDE) return HXG_ERR_TOO_LARGE;
+  // an error left by the caller's earlier work would surface in this
+  // call's launch checks after part of the work is queued: refuse first
+  if (cudaPeekAtLastError() != cudaSuccess) return HXG_ERR_CUDA;
   double *scratch = nullptr;
-  int st = scratch_for_current_device(&scratch);
+  int st = scratch_for_current_context(&scratch);
   if (st != HXG_OK) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double *tmp[5];

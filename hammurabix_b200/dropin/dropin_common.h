@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
+#include <cstring>
 #include <stdexcept>
 #include <string>
 #include <typeinfo>
@@ -28,12 +29,76 @@ inline void check(int st, hxg_handle *h, const char *what) {
   }
 }
 
+// What a device slot holds: the host arrays it was uploaded from (or
+// downloaded into), their geometry and a fingerprint of their contents.  A
+// host address alone does not identify a grid: a second Pipeline in the
+// same process can get a recycled address for a new Grid_* array, and a
+// caller can rewrite an array in place between runs (a sampling loop), so
+// an upload is skipped only when all three match.
+struct SlotKey {
+  bool valid = false;
+  const void *ptr[3] = {nullptr, nullptr, nullptr};
+  hxg_grid_desc_t desc{};
+  uint64_t fp[3] = {0, 0, 0};
+};
+
+inline bool same_desc(const hxg_grid_desc_t &a, const hxg_grid_desc_t &b) {
+  return a.nx == b.nx && a.ny == b.ny && a.nz == b.nz && a.nE == b.nE && a.x_min == b.x_min &&
+         a.x_max == b.x_max && a.y_min == b.y_min && a.y_max == b.y_max &&
+         a.z_min == b.z_min && a.z_max == b.z_max && a.E_min == b.E_min &&
+         a.E_max == b.E_max && a.E_fact == b.E_fact;
+}
+
+inline bool same_key(const SlotKey &a, const SlotKey &b) {
+  if (!a.valid || !b.valid || !same_desc(a.desc, b.desc)) return false;
+  for (int k = 0; k < 3; ++k)
+    if (a.ptr[k] != b.ptr[k] || a.fp[k] != b.fp[k]) return false;
+  return true;
+}
+
+// Content fingerprint of n doubles: the sum over 8-byte words of a mixed
+// hash of (word, index) -- the splitmix64 finaliser (Steele, Lea & Flood,
+// OOPSLA 2014) -- so a change of any word or a swap of two words changes
+// it.  Summed by all host threads: bound by host memory bandwidth.
+inline uint64_t fingerprint(const double *p, size_t n) {
+  if (p == nullptr) return 0;
+  uint64_t acc = 0;
+#pragma omp parallel for reduction(+ : acc) schedule(static)
+  for (long long i = 0; i < (long long)n; ++i) {
+    uint64_t x;
+    std::memcpy(&x, p + i, sizeof(x));
+    x ^= 0x9E3779B97F4A7C15ull * (uint64_t)(i + 1);
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    acc += x ^ (x >> 31);
+  }
+  return acc ^ (uint64_t)n;
+}
+
+inline size_t values_per_component(const hxg_grid_desc_t &d) {
+  return (size_t)d.nx * d.ny * d.nz * (d.nE ? d.nE : 1);
+}
+
+inline SlotKey key_of(const hxg_grid_desc_t &d, const double *x, const double *y,
+                      const double *z) {
+  SlotKey k;
+  k.valid = true;
+  k.desc = d;
+  const double *c[3] = {x, y, z};
+  const size_t n = values_per_component(d);
+  for (int j = 0; j < 3; ++j) {
+    k.ptr[j] = c[j];
+    k.fp[j] = fingerprint(c[j], n);
+  }
+  return k;
+}
+
 // One device handle per process, re-used across frequency passes
 // (Pipeline::assemble_obs calls write_grid once per <sync> entry).
 struct DeviceState {
   hxg_handle *h = nullptr;
   int precision = HXG_FP64;
-  const void *uploaded[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  SlotKey slots[5];
   ~DeviceState() {
     if (h) hxg_destroy(h);
   }
@@ -66,11 +131,22 @@ inline hxg_grid_desc_t desc_of(const P &g) {
   return d;
 }
 
+// Uploads the host arrays into the slot unless it already holds exactly
+// these contents at this geometry.
 inline void upload_vec(DeviceState &s, int slot, const hxg_grid_desc_t &d,
                        const double *x, const double *y, const double *z) {
-  if (s.uploaded[slot] == x) return;
+  const SlotKey k = key_of(d, x, y, z);
+  if (same_key(k, s.slots[slot])) return;
+  s.slots[slot].valid = false;
   check(hxg_upload_grid(s.h, slot, &d, x, y, z), s.h, "hxg_upload_grid");
-  s.uploaded[slot] = x;
+  s.slots[slot] = k;
+}
+
+// Records that the slot's device contents were copied into these host
+// arrays (a device generator's output).
+inline void mark_resident(DeviceState &s, int slot, const hxg_grid_desc_t &d,
+                          const double *x, const double *y, const double *z) {
+  s.slots[slot] = key_of(d, x, y, z);
 }
 
 // The regular-field part of the reference's model selection
@@ -105,7 +181,17 @@ inline void map_breg(DeviceState &s, const Breg *breg, const Grid_breg *gbreg,
       d.bss = j.bss;
       d.ring = j.ring;
       d.bar = j.bar;
-      d.arm_num = (uint32_t)std::min<std::size_t>(j.arm_num, 8);
+      // Param reads a phase and an amplitude for four arms
+      // (param.cc:207-227); more arms than it holds, or than the device
+      // block holds, would be read past the end (the reference reads past
+      // its vectors): refused
+      if (j.arm_num > j.arm_amp.size() || j.arm_num > j.arm_phi0.size() || j.arm_num > 8)
+        throw std::runtime_error("hammurabiX-B200: Breg_jaffe arm_num " +
+                                 std::to_string(j.arm_num) + " exceeds the " +
+                                 std::to_string(std::min<std::size_t>(
+                                     8, std::min(j.arm_amp.size(), j.arm_phi0.size()))) +
+                                 " arms given");
+      d.arm_num = static_cast<uint32_t>(j.arm_num);
       d.disk_amp = j.disk_amp;
       d.disk_z0 = j.disk_z0;
       d.halo_amp = j.halo_amp;

@@ -42,7 +42,7 @@ void Brnd_es::write_grid(const Param *par, const Breg *breg, const Grid_breg *gb
   check(hxg_generate_brnd_es(s.h, &d, &p, obs, par->brnd_seed), s.h, "hxg_generate_brnd_es");
   check(hxg_download_grid(s.h, HXG_FIELD_BRND, grid->bx.get(), grid->by.get(), grid->bz.get()),
         s.h, "hxg_download_grid");
-  s.uploaded[HXG_FIELD_BRND] = grid->bx.get();
+  mark_resident(s, HXG_FIELD_BRND, d, grid->bx.get(), grid->by.get(), grid->bz.get());
 }
 
 // Brnd_es::spectrum (brnd_es.cc:34-49): broken power law in k (1/kpc)
@@ -76,7 +76,7 @@ void TErnd_dft::write_grid(const Param *par, const TEreg *, const Grid_tereg *,
         "hxg_generate_ternd_dft");
   check(hxg_download_grid(s.h, HXG_FIELD_TERND, grid->te.get(), nullptr, nullptr), s.h,
         "hxg_download_grid");
-  s.uploaded[HXG_FIELD_TERND] = grid->te.get();
+  mark_resident(s, HXG_FIELD_TERND, d, grid->te.get(), nullptr, nullptr);
 }
 
 // TErnd_dft::spectrum (ternd_dft.cc:17-24): zero below k0

@@ -59,12 +59,7 @@ hxg_models_t map_models(DeviceState &s, const Breg *breg, const Brnd *,
   // regular n_e
   if (par->grid_tereg.read_permission) {
     m.tereg = HXG_TEREG_GRID;
-    if (s.uploaded[HXG_FIELD_TEREG] != gtereg->te.get()) {
-      const hxg_grid_desc_t d = desc_of(par->grid_tereg);
-      check(hxg_upload_grid(s.h, HXG_FIELD_TEREG, &d, gtereg->te.get(), nullptr, nullptr),
-            s.h, "hxg_upload_grid");
-      s.uploaded[HXG_FIELD_TEREG] = gtereg->te.get();
-    }
+    upload_vec(s, HXG_FIELD_TEREG, desc_of(par->grid_tereg), gtereg->te.get(), nullptr, nullptr);
   } else if (par->grid_tereg.build_permission) {
     if (dynamic_cast<const TEreg_unif *>(tereg)) {
       m.tereg = HXG_TEREG_UNIF;
@@ -82,27 +77,18 @@ hxg_models_t map_models(DeviceState &s, const Breg *breg, const Brnd *,
   // random n_e (ternd.cc:12-19)
   if (par->grid_ternd.read_permission or par->grid_ternd.build_permission) {
     m.ternd = HXG_TERND_GRID;
-    if (s.uploaded[HXG_FIELD_TERND] != gternd->te.get()) {
-      const hxg_grid_desc_t d = desc_of(par->grid_ternd);
-      check(hxg_upload_grid(s.h, HXG_FIELD_TERND, &d, gternd->te.get(), nullptr, nullptr),
-            s.h, "hxg_upload_grid");
-      s.uploaded[HXG_FIELD_TERND] = gternd->te.get();
-    }
+    upload_vec(s, HXG_FIELD_TERND, desc_of(par->grid_ternd), gternd->te.get(), nullptr, nullptr);
   }
   // cosmic-ray electrons
   if (par->grid_cre.read_permission) {
     // CRE_num: spectral integral over the CRE grid (integrator.cc:288-330)
     m.cre = HXG_CRE_GRID;
-    if (s.uploaded[HXG_FIELD_CRE] != gcre->cre_flux.get()) {
-      hxg_grid_desc_t d = desc_of(par->grid_cre);
-      d.nE = static_cast<uint32_t>(par->grid_cre.nE);
-      d.E_min = par->grid_cre.E_min;
-      d.E_max = par->grid_cre.E_max;
-      d.E_fact = par->grid_cre.E_fact;
-      check(hxg_upload_grid(s.h, HXG_FIELD_CRE, &d, gcre->cre_flux.get(), nullptr, nullptr),
-            s.h, "hxg_upload_grid");
-      s.uploaded[HXG_FIELD_CRE] = gcre->cre_flux.get();
-    }
+    hxg_grid_desc_t d = desc_of(par->grid_cre);
+    d.nE = static_cast<uint32_t>(par->grid_cre.nE);
+    d.E_min = par->grid_cre.E_min;
+    d.E_max = par->grid_cre.E_max;
+    d.E_fact = par->grid_cre.E_fact;
+    upload_vec(s, HXG_FIELD_CRE, d, gcre->cre_flux.get(), nullptr, nullptr);
   } else if (dynamic_cast<const CRE_ana *>(cre)) {
     m.cre = HXG_CRE_ANA;
     m.cre_ana = {par->cre_ana.alpha, par->cre_ana.beta, par->cre_ana.theta,
@@ -166,10 +152,17 @@ struct PassCache {
   std::vector<hxg_obs_t> obs;                       // predicted later passes
   std::vector<std::array<std::vector<double>, 5>> maps;
   hxg_models_t models{};
-  const void *uploaded[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  SlotKey slots[5];  // what the device slots held when the maps were made
   std::vector<double> mask;
   void clear() { obs.clear(); maps.clear(); }
 };
+
+// Slots compare equal when both are empty or both hold the same contents.
+bool same_slots(const SlotKey a[5], const SlotKey b[5]) {
+  for (int j = 0; j < 5; ++j)
+    if ((a[j].valid || b[j].valid) && !same_key(a[j], b[j])) return false;
+  return true;
+}
 
 PassCache &pass_cache() {
   static PassCache c;
@@ -213,7 +206,7 @@ void Integrator::write_grid(const Breg *breg, const Brnd *brnd,
   for (size_t k = 0; k < pc.obs.size(); ++k) {
     if (std::memcmp(&pc.obs[k], &o, sizeof(o)) != 0 ||
         std::memcmp(&pc.models, &m, sizeof(m)) != 0 ||
-        std::memcmp(pc.uploaded, s.uploaded, sizeof(pc.uploaded)) != 0 || pc.mask != mk)
+        !same_slots(pc.slots, s.slots) || pc.mask != mk)
       continue;
     publish(pc.maps[k]);
     pc.obs.erase(pc.obs.begin() + k);
@@ -257,7 +250,7 @@ void Integrator::write_grid(const Breg *breg, const Brnd *brnd,
     pc.obs.assign(passes.begin() + 1, passes.end());
     pc.maps.assign(maps.begin() + 1, maps.end());
     pc.models = m;
-    std::memcpy(pc.uploaded, s.uploaded, sizeof(pc.uploaded));
+    for (int j = 0; j < 5; ++j) pc.slots[j] = s.slots[j];
     pc.mask = mk;
   }
   publish(maps[0]);

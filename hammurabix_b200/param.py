@@ -279,6 +279,10 @@ class Param:
         j.bar_b = _f(s, "bar_b") * U.kpc
         j.bar_phi0 = _f(s, "bar_phi0") * U.rad
         j.arm_num = _u(s, "arm_num")
+        # Param reads four arms (param.cc:207-227); more would be read past
+        # its vectors
+        if j.arm_num > 4:
+            raise ParamError(f"Breg_jaffe arm_num {j.arm_num} exceeds the 4 arms given")
         j.arm_r0 = _f(s, "arm_r0") * U.kpc
         j.arm_z0 = _f(s, "arm_z0") * U.kpc
         for i in range(4):

@@ -465,11 +465,18 @@ int hxg_get_launch_count(hxg_handle *h, int64_t *count);
  *    masks (do_mask) return HXG_ERR_UNSUPPORTED.
  *  - work is queued on `stream` (cudaStream_t; NULL = legacy default) of
  *    the current device; the call does not synchronise.
- *  - the first call on a device looks the scratch address up on that
- *    device (cudaGetSymbolAddress); make that first call before any stream
- *    capture.  All calls share the scratch and it keeps the last call's
- *    contents; calls whose GPU work overlaps (other streams, other threads)
- *    race on it, so serialise them.                                        */
+ *  - the first call in a CUDA context (per device, for runtime-API
+ *    callers: its primary context) looks the scratch address up there
+ *    (cudaGetSymbolAddress); make that first call before any stream
+ *    capture.  A device reset (cudaDeviceReset) makes a new context, and
+ *    the next call looks the address up again; a failed lookup is retried
+ *    on the next call.
+ *  - an error already pending in the CUDA runtime (cudaPeekAtLastError)
+ *    makes the call return HXG_ERR_CUDA before it queues any work; when
+ *    the call returns HXG_ERR_CUDA the outputs are undefined.
+ *  - all calls share the scratch and it keeps the last call's contents;
+ *    calls whose GPU work overlaps (other streams, other threads) race on
+ *    it, so serialise them.                                                */
 #define HXG_NOALLOC_MAX_NSIDE 128
 int hxg_write_grid_noalloc(const hxg_obs_t *obs, const hxg_models_t *models,
                            const hxg_grid_desc_t *grid,

@@ -64,3 +64,18 @@ def rel_err(a, b):
     if s == 0.0:
         return d
     return d / s
+
+
+def point_err(a, b, floor=1e-3):
+    """max |a - b| / |b| over the pixels where |b| > floor * max |b|: the
+    pointwise relative error of a map away from its zero crossings (Q and U
+    oscillate through zero, where a relative error means nothing)."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    if b.size == 0:
+        return 0.0
+    s = np.abs(b).max()
+    if s == 0.0:
+        return np.abs(a - b).max()
+    sel = np.abs(b) > floor * s
+    return float((np.abs(a - b)[sel] / np.abs(b[sel])).max())

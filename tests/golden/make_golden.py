@@ -25,7 +25,7 @@ that holds the hammurabiX source tree; the outputs are committed).
    DFT (oracle/shim), i.e. the deviates the device generators draw; each
    case's hxg_models_t block is stored beside its field.
 
-Usage: python tests/golden/make_golden.py [hammurabiX source dir]
+Usage: python tests/golden/make_golden.py <hammurabiX source dir>
 """
 import os
 import shutil
@@ -142,7 +142,9 @@ def reference_rfg(src):
 
 
 if __name__ == "__main__":
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <hammurabiX source dir>")
+    src = sys.argv[1]
     reference_fixtures(src)
     reference_maps()
     reference_models_ext(src)

@@ -272,3 +272,105 @@ def test_dropin_generators_match_reference_cli(tmp_path, fields, cells):
         tol = 1e-10 if k in ("dm.bin", "fd.bin") else 1e-9
         assert rel_err(out["gpu"][k], out["ref"][k]) <= tol, (k, rel_err(out["gpu"][k],
                                                                         out["ref"][k]))
+
+
+# Random B generators the B200 build does not replace (Brnd_jf12,
+# source/field/b/brnd_jf12.cc:137-211; Brnd_mhd, brnd_mhd.cc:15-135): the
+# drop-in CLI has no GSL or FFTW behind them, so it must stop with an error
+# instead of running them on stand-ins.
+_BRND_ES = XML_RND[XML_RND.index('    <random cue="{bcue}"'):XML_RND.index("  </magneticfield>")]
+_BRND_OTHER = {
+    "jf12": """    <random cue="1" type="global" seed="7">
+      <global type="jf12">
+        <jf12>
+          <rms value="1.0"/><k0 value="10.0"/><k1 value="0.1"/><a0 value="1.7"/>
+          <a1 value="0.0"/><rho value="1.0"/>
+          <b0_1 value="10.81"/><b0_2 value="6.96"/><b0_3 value="9.59"/><b0_4 value="6.96"/>
+          <b0_5 value="1.96"/><b0_6 value="16.34"/><b0_7 value="37.29"/><b0_8 value="10.35"/>
+          <b0_int value="7.63"/><z0_spiral value="0.61"/>
+          <b0_halo value="4.68"/><r0_halo value="10.97"/><z0_halo value="2.84"/>
+        </jf12>
+      </global>
+    </random>
+""",
+    "mhd": """    <random cue="1" type="local" seed="7">
+      <local type="mhd">
+        <mhd>
+          <pa0 value="1"/><pf0 value="1"/><ps0 value="1"/><k0 value="10.0"/>
+          <aa0 value="1.7"/><af0 value="1.5"/><as0 value="1.7"/><k1 value="0.1"/>
+          <a1 value="0.0"/><beta value="0.1"/><ma value="0.5"/>
+        </mhd>
+      </local>
+    </random>
+""",
+}
+
+
+@pytest.mark.parametrize("kind", sorted(_BRND_OTHER))
+def test_dropin_refuses_unreplaced_generators(tmp_path, kind):
+    """The generator throws before any device work, so this runs without a
+    GPU: the process exits non-zero and names the missing replacement."""
+    if not os.path.exists(HAMX_B200):
+        pytest.skip("drop-in binary not built")
+    xml = XML_RND.replace(_BRND_ES, _BRND_OTHER[kind]).format(d=str(tmp_path), bcue=1, tcue=0)
+    path = tmp_path / "params.xml"
+    path.write_text(xml)
+    r = subprocess.run([HAMX_B200, str(path)], capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0
+    assert "not replaced on the B200 build" in r.stderr, r.stdout + r.stderr
+    assert not (tmp_path / "dm.bin").exists()
+
+
+def test_dropin_links_no_oracle_code():
+    """The drop-in CLI is product code: none of the oracle's stand-ins (its
+    GSL/FFTW shim, cell-stream RNG, direct-sum DFT) are linked into it."""
+    if not os.path.exists(HAMX_B200):
+        pytest.skip("drop-in binary not built")
+    r = subprocess.run(["nm", "-C", HAMX_B200], capture_output=True, text=True, check=True)
+    syms = r.stdout
+    for marker in ("hxo_", "philox", "splitmix", "cells_for_next_seed"):
+        assert marker not in syms, marker
+    assert "fftw_execute_dft" in syms and "gsl_rng_alloc" in syms
+
+
+HAMX_B200_MULTI = os.path.join(ROOT, "hammurabix_b200", "dropin", "_build", "hamx_b200_multi")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_dropin_second_pipeline_sees_new_grids(tmp_path, fields32, precision):
+    """Two Pipelines in one process (hamx_b200_multi), each reading its own
+    grid files of the same size: the second run's Grid_* arrays are new
+    allocations of the same size, which the allocator can hand out at the
+    first run's addresses, and its grids differ from the first run's.  Each
+    run must match the reference CLI on its own inputs; a device slot or a
+    kept FP32C pass keyed on host addresses alone would give the second run
+    the first run's maps."""
+    if not (os.path.exists(HAMX_REF) and os.path.exists(HAMX_B200_MULTI)):
+        pytest.skip("reference CLI or multi-run drop-in not built")
+    bx, by, bz, ne = fields32
+    second = (-0.7 * np.asarray(by), 1.3 * np.asarray(bx), np.asarray(bz)[::-1].copy(),
+              0.5 * np.asarray(ne)[::-1].copy())
+    runs = [("a", fields32), ("b", second)]
+    xmls, ref = [], {}
+    for name, f in runs:
+        rd = tmp_path / f"ref_{name}"
+        gd = tmp_path / f"gpu_{name}"
+        rd.mkdir()
+        gd.mkdir()
+        ref[name] = _run(HAMX_REF, str(rd), _write_inputs(str(rd), f, None))
+        xmls.append(_write_inputs(str(gd), f, None))
+    env = dict(os.environ, HAMMURABIX_PRECISION=precision)
+    r = subprocess.run([HAMX_B200_MULTI] + xmls, capture_output=True, text=True, timeout=600,
+                       env=env)
+    assert r.returncode == 0, r.stdout + r.stderr
+    for name, _ in runs:
+        got = {k: np.fromfile(str(tmp_path / f"gpu_{name}" / k)) for k in OUTPUTS}
+        for k in OUTPUTS:
+            if precision == "fp64":
+                tol = 1e-10 if k in ("dm.bin", "fd.bin") else 1e-9
+            else:
+                tol = 1e-5
+            assert rel_err(got[k], ref[name][k]) <= tol, (name, k, rel_err(got[k], ref[name][k]))
+    # the two runs' maps really differ, so a stale slot could not pass
+    assert rel_err(ref["a"]["dm.bin"], ref["b"]["dm.bin"]) > 1e-3

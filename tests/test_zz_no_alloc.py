@@ -48,6 +48,9 @@ def test_noalloc_matches_write_grid(fields32):
     for call in range(2):
         for o, exp in zip(passes, expect):
             out = _outputs(torch, o)
+            # the outputs and records were written on torch's stream; the
+            # entry point's stream must not start before those writes land
+            stream.wait_stream(torch.cuda.current_stream())
             st = lib.hxg_write_grid_noalloc(
                 C.byref(o), C.byref(models), C.byref(desc), _vp(rec),
                 *(_vp(out[k]) for k in KEYS), C.c_void_p(stream.cuda_stream))
