@@ -35,18 +35,19 @@ BYTES_PER_SAMPLE = {"fp32c": 128, "fp64": 256}  # 8 corners x 4 gridded componen
 
 WORKLOADS = {
     "config3": dict(nside_shells=[128, 256, 512, 1024], r_max_kpc=30.0, res_kpc=0.01,
-                    freqs_ghz=[0.408, 1.4, 30.0], grid_n=512, seeds=(3, 4),
-                    cpu_sample_shells=[8, 16, 32, 64]),
+                    freqs_ghz=[0.408, 1.4, 30.0], grid_n=512, seeds=(3, 4)),
     "small": dict(nside_shells=[32, 64, 128, 256], r_max_kpc=30.0, res_kpc=0.01,
-                  freqs_ghz=[0.408, 1.4, 30.0], grid_n=128, seeds=(3, 4),
-                  cpu_sample_shells=[4, 8, 16, 32]),
+                  freqs_ghz=[0.408, 1.4, 30.0], grid_n=128, seeds=(3, 4)),
     # the case kernel captures run on: grid records (268 MB FP32) above L2,
     # an Nside-512 outer shell (one lane per pixel, as the config-3 outer
     # shells), about 15 ms per launch
     "profile": dict(nside_shells=[64, 128, 256, 512], r_max_kpc=30.0, res_kpc=0.01,
-                    freqs_ghz=[0.408, 1.4, 30.0], grid_n=256, seeds=(3, 4),
-                    cpu_sample_shells=[4, 8, 16, 32]),
+                    freqs_ghz=[0.408, 1.4, 30.0], grid_n=256, seeds=(3, 4)),
 }
+# The bounded sample both arms time like for like: the first frequency pass
+# (DM + FD + synchrotron) of the workload over its two innermost shells
+# only, with their own radii, Nsides and sample positions, on the same grids.
+SUB_SHELLS = 2
 
 
 def log(*a):
@@ -62,14 +63,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_sample(name):
-    """Bytes of DRAM traffic per LOS sample of the integration kernel from
-    the committed ncu summary (profiles/<name>), or None."""
+def profile_figure(name, key):
+    """A figure of the integration kernel from the committed ncu summary
+    profiles/<name>: the number on its line '<key>: <value>', or None."""
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("dram_bytes_per_sample:"):
+        if line.startswith(key + ":"):
             return float(line.split(":", 1)[1].split()[0])
     return None
 
@@ -148,38 +149,77 @@ def make_passes(wl, nside_shells=None):
                          wl["freqs_ghz"])
 
 
+def sub_workload(wl):
+    """Obs of the bounded sample: pass 1 of the workload restricted to its
+    SUB_SHELLS innermost shells (the same shell radii, Nsides and radial
+    steps), output maps at the outermost of those Nsides."""
+    from hammurabix_b200 import workloads as W
+    full = make_passes(wl)[0]
+    o = W.make_obs(wl["nside_shells"][:SUB_SHELLS], wl["r_max_kpc"], wl["res_kpc"],
+                   freq_ghz=full.sync_freq / 1e9)
+    for i in range(SUB_SHELLS + 1):
+        o.radii_shell[i] = full.radii_shell[i]
+    return o
+
+
+def sub_workload_text(wl):
+    from hammurabix_b200 import workloads as W
+    from hammurabix_b200 import units as U
+    o = sub_workload(wl)
+    shells = "/".join(str(o.nside_shell[i]) for i in range(o.total_shell))
+    return (f"pass 1 ({o.sync_freq / 1e9:g} GHz with DM + FD) over the workload's {SUB_SHELLS} "
+            f"innermost shells (Nside {shells}, 0-{o.radii_shell[SUB_SHELLS] / U.kpc:g} kpc), "
+            f"same {wl['grid_n']}^3 grids: {W.samples_of(o)} LOS samples, "
+            f"Integrator::write_grid only")
+
+
 def cpu_baseline(wl, host_fields, steps=1):
     """The reference's FP64 OpenMP integrator (oracle/_ref, compiled from the
-    reference sources) on a bounded sample: the workload's geometry, grids and
-    first frequency pass at 1/16 of its angular resolution, all host cores."""
+    reference sources) on the bounded sample (sub_workload), all host cores:
+    an exact subset of the workload's samples, which the GPU forms also time."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     from hammurabix_b200 import workloads as W
     ref = pyoracle.Reference()
     threads = os.cpu_count()
-    o = make_passes(wl, wl["cpu_sample_shells"])[0]
-    n = wl["grid_n"]
-    grids = W.grids_dict(n, *host_fields)
+    o = sub_workload(wl)
+    grids = W.grids_dict(wl["grid_n"], *host_fields)
     m = W.grid_models()
-    samples = W.samples_of(o)
     times = []
     for _ in range(steps):
         _, secs = ref.write_grid(o, m, grids, nthreads=threads)
         times.append(secs)
-    return {"samples": samples, "seconds": times, "threads": threads,
-            "sample": (f"pass 1 ({o.sync_freq / 1e9:g} GHz with DM+FD) of the workload at "
-                       f"Nside {'/'.join(str(s) for s in wl['cpu_sample_shells'])}, "
-                       f"same {n}^3 grids, {samples} LOS samples; Integrator::write_grid only")}
+    return {"samples": W.samples_of(o), "seconds": times, "threads": threads,
+            "sample": sub_workload_text(wl)}
+
+
+def config_of(args, wl, ws, shard):
+    """The workload's config entry, the same for both arms."""
+    n = wl["grid_n"]
+    passes = make_passes(wl)
+    from hammurabix_b200 import workloads as W
+    return {"workload": f"{args.workload}: Nside "
+                        f"{'/'.join(str(s) for s in wl['nside_shells'])} x "
+                        f"{len(wl['nside_shells'])} shells to {wl['r_max_kpc']:g} kpc, "
+                        f"{wl['res_kpc']} kpc steps, {n}^3 FP32 grids, "
+                        f"{'/'.join(str(f) for f in wl['freqs_ghz'])} GHz",
+            "samples_per_step": sum(W.samples_of(o) for o in passes),
+            "passes_per_step": len(passes),
+            "l2": f"inputs larger than L2 (grids {4 * 4 * n ** 3 / 1e9:.2f} GB FP32)",
+            "parallelism": (f"shell pixels split over {ws} GPUs, FD all-reduce per shell"
+                            if shard else f"replicas x{ws}" if ws > 1 else "1 GPU")}
 
 
 def run_reference_arm(args, wl):
+    """The reference's own CPU integrator on the workload's config: each
+    step is one Integrator::write_grid of the bounded sample (sub_workload)
+    on all host cores; the value is its LOS samples/s."""
     # CPU only: no process group is needed; rank 0 alone runs and prints
     from hammurabix_b200 import replicas
+    from hammurabix_b200 import workloads as W
     ws, rank, _ = replicas.env()
     if rank != 0:
         return
-    import numpy as np
-    from hammurabix_b200 import workloads as W
     b = W.random_grids_torch(wl["grid_n"], *wl["seeds"], device="cpu")
     host = [t.double().numpy().reshape(-1) for t in b]
     del b
@@ -190,9 +230,9 @@ def run_reference_arm(args, wl):
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": args.workload + " (bounded sample)",
-                                        "sample": cb["sample"]},
+        "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_of(args, wl, ws, ws > 1 and args.mode == "shard"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cb["threads"],
                          "kind": "reference", "sample": cb["sample"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -282,11 +322,24 @@ def adjoint_ratio(args, dev, stream, torch):
         if it > 0:
             fwd.append(ev[0].elapsed_time(ev[1]))
             adj.append(ev[1].elapsed_time(ev[2]))
+    # the same forward without the checkpoint stores
+    ig.set_checkpointing(False)
+    plain = []
+    for it in range(1 + args.adjoint_steps):
+        torch.cuda.synchronize(dev)
+        ev[0].record(stream)
+        ig.write_grid_device(o, *outs)
+        ev[1].record(stream)
+        torch.cuda.synchronize(dev)
+        if it > 0:
+            plain.append(ev[0].elapsed_time(ev[1]))
     ig.close()
-    f, a = sum(fwd) / len(fwd), sum(adj) / len(adj)
+    f, a, fp = sum(fwd) / len(fwd), sum(adj) / len(adj), sum(plain) / len(plain)
     return {"workload": "config4: Nside 64/128/256 x 3 shells to 30 kpc, 256^3 FP64 grids, "
                         "23 GHz + DM + FD, FP64 form",
             "forward_ms": f, "adjoint_ms": a, "ratio": a / f,
+            "forward_plain_ms": fp, "ratio_vs_plain_forward": a / fp,
+            "checkpoint_overhead": f / fp - 1.0,
             "samples": W.samples_of(o)}
 
 
@@ -371,6 +424,9 @@ def main():
     ap.add_argument("--workload", default="config3", choices=sorted(WORKLOADS))
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--e2e64-steps", type=int, default=3)
+    ap.add_argument("--sub-steps", type=int, default=5,
+                    help="timed repetitions of the bounded sample in each GPU form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=2)
     ap.add_argument("--batch-steps", type=int, default=2)
@@ -538,9 +594,36 @@ def main():
         del out64
         log(f"[rank {rank}] fp64: {ms64:.1f} ms/step; errors {errs}")
 
+    # ---- the bounded sample, timed like for like with the CPU reference -----------
+    sub = None
+    if args.sub_steps > 0 and not shard:
+        osub = sub_workload(wl)
+        nsub = abi.npix(osub.nside_dm)
+        sub = {"sample": sub_workload_text(wl), "samples": W.samples_of(osub),
+               "valid_samples": sum(W.valid_samples(osub))}
+        for prec in ("fp64", "fp32c"):
+            ig_ = make_integ(prec)
+            m5 = [torch.zeros(nsub, dtype=torch.float64, device=dev) for _ in range(5)]
+            ig_.write_grid_device(osub, *m5)
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            barrier()
+            ev0.record(stream)
+            for _ in range(args.sub_steps):
+                ig_.write_grid_device(osub, *m5)
+            ev1.record(stream)
+            barrier()
+            ms = ev0.elapsed_time(ev1) / args.sub_steps
+            ig_.close()
+            sub[f"{prec}_ms"] = ms
+            sub[f"{prec}_samples_per_s"] = sub["samples"] / (ms / 1e3)
+        log(f"[rank {rank}] bounded sample: {sub}")
+
     # ---- end to end through the host-buffer C ABI -----------------------------
-    e2e = None
-    if args.e2e_steps > 0:
+    def e2e_leg(prec, nsteps_timed):
+        """Step throughput through the host-buffer C ABI in form `prec`:
+        every step uploads its grids from pinned host memory and reads its
+        maps back inside the timed region."""
         pinned = [torch.empty(t.numel(), dtype=torch.float64, pin_memory=True) for t in f64]
         for p, t in zip(pinned, f64):
             p.copy_(t)
@@ -548,7 +631,7 @@ def main():
         keys = ("dm", "fd", "is", "qs", "us")
 
         def e2e_integ(s):
-            ig_ = Integrator("fp32c", device=local)
+            ig_ = Integrator(prec, device=local)
             ig_.set_stream(s.cuda_stream)
             ig_.set_models(models)
             return ig_
@@ -617,13 +700,13 @@ def main():
         e2e_run(2)
         barrier()
         te0 = time.perf_counter()
-        e2e_run(args.e2e_steps)
+        e2e_run(nsteps_timed)
         barrier()
-        te = max_over_ranks((time.perf_counter() - te0) / args.e2e_steps)
+        te = max_over_ranks((time.perf_counter() - te0) / nsteps_timed)
         h2d = sum(h.nbytes for h in hosts)
         d2h = sum(8 * (abi.npix(o.nside_dm) * o.do_dm + abi.npix(o.nside_fd) * o.do_fd
                        + 3 * abi.npix(o.nside_sync)) for o in passes)
-        e2e = {"value": (1 if shard else ws) * samples_step / te, "unit": UNIT,
+        res = {"value": (1 if shard else ws) * samples_step / te, "unit": UNIT,
                "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": te * 1e3,
                "overlap": ("two handles on two streams and a read-back stream: step k+1's "
@@ -632,7 +715,13 @@ def main():
         for ig_ in iges:
             ig_.close()
         del pinned, hosts, pinned_outs
-        log(f"[rank {rank}] e2e: {te * 1e3:.1f} ms/step")
+        log(f"[rank {rank}] e2e {prec}: {te * 1e3:.1f} ms/step")
+        return res
+
+    e2e = e2e_leg("fp32c", args.e2e_steps) if args.e2e_steps > 0 else None
+    # the FP64 form end to end: the like-for-like counterpart of the
+    # reference's FP64 integrator
+    e2e64 = e2e_leg("fp64", args.e2e64_steps) if args.e2e64_steps > 0 else None
 
     # ---- adjoint / forward cost on the config-4 workload (FP64 form) -------
     adjoint = None
@@ -653,25 +742,47 @@ def main():
         log(f"[rank {rank}] generators: {rfg}")
 
     # ---- roofline of the shell-integration kernel -------------------------------
-    peak, peak_kind = measured_peaks()
+    # The kernel re-reads its voxels from L1/L2 (neighbouring samples and rays
+    # share cells), so HBM is far from its roof; what bounds it is
+    # instruction issue: one warp instruction per clock per SM sub-partition.
+    # achieved = (warp instructions per integrated sample, from the ncu
+    # capture of this kernel on this workload) x (integrated samples per
+    # second of kernel time); integrated = passing the r / z cuts.
+    peak_hbm, peak_kind = measured_peaks()
     per_launch_s = kms / 1e3 / max(klaunch, 1)
     samples_per_launch = ksamples / max(klaunch, 1)
-    achieved = samples_per_launch * BYTES_PER_SAMPLE["fp32c"] / per_launch_s / 1e9
     fused = len(passes) in (2, 3)
     kname = (f"hxg::shell_fp32c_multi_kernel<1,false,{len(passes)},true>" if fused
              else "hxg::shell_fp32c_kernel<1,false,true>")
-    tps = traffic_per_sample("shell_fp32c_multi_config3.md" if fused
-                             else "shell_fp32c_config3.md")
+    prof_name = "shell_fp32c_multi_config3.md" if fused else "shell_fp32c_config3.md"
+    tps = profile_figure(prof_name, "dram_bytes_per_sample")
+    ipv = profile_figure(prof_name, "warp_inst_per_valid_sample")
+    # one traversal per shell serves all fused passes: its integrated samples
+    # are those of one pass; launched one by one, every pass traverses
+    valid_trav = sum(W.valid_samples(passes[0])) * (1 if fused else len(passes))
+    valid_per_s = valid_trav * args.steps / (kms / 1e3) if kms > 0 else None
+    clk_sum = clk.summary()
+    mhz = clk_sum["sm_mhz"] if clk_sum else 1965.0
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    issue_peak = 4 * sms * mhz * 1e6 / 1e9          # G warp instructions / s
+    achieved = ipv * valid_per_s / 1e9 if (ipv and valid_per_s) else None
     traffic = (tps * samples_per_launch) if tps else None
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                "dram_gbs": traffic / per_launch_s / 1e9 if traffic else None,
-                "note": "achieved counts the 8-corner gather of the grid interpolation "
-                        f"({BYTES_PER_SAMPLE['fp32c']} B per reference LOS sample); consecutive "
-                        "samples of a ray re-read the same voxels from L1/L2 and the fused "
-                        "kernel gathers once for the step's frequency passes, so DRAM traffic "
-                        "stays far below it and the kernel is bound by instruction issue, "
-                        "not HBM",
+    dram_gbs = traffic / per_launch_s / 1e9 if traffic else None
+    roofline = {"bound": "issue", "achieved": achieved, "peak": issue_peak,
+                "unit": "G warp instructions/s",
+                "frac": achieved / issue_peak if achieved else None,
+                "peak_kind": f"4 warp instructions per clock per SM x {sms} SMs x "
+                             f"{mhz:g} MHz (median sampled SM clock)",
+                "warp_inst_per_valid_sample": ipv,
+                "valid_samples_per_s": valid_per_s,
+                "traffic": traffic, "dram_gbs": dram_gbs,
+                "dram_frac": dram_gbs / peak_hbm if dram_gbs else None,
+                "hbm_peak_gbs": peak_hbm, "hbm_peak_kind": peak_kind,
+                "gather_gbs": samples_per_launch * BYTES_PER_SAMPLE["fp32c"] / per_launch_s / 1e9,
+                "note": "bound: instruction issue. gather_gbs counts the 8-corner gather "
+                        f"({BYTES_PER_SAMPLE['fp32c']} B per reference loop iteration), served "
+                        "from L1/L2; traffic / dram_gbs / dram_frac are the DRAM bytes the "
+                        "kernel moves (ncu) against the measured HBM copy bandwidth",
                 "kernel": kname,
                 "kernel_share_of_step": (kms / 1e3) / t32 if t32 > 0 else None,
                 "kernel_samples_per_s": ksamples / (kms / 1e3) if kms > 0 else None}
@@ -683,6 +794,11 @@ def main():
         v = cb["samples"] / cb["seconds"][0]
         cpu = {"value": v, "unit": UNIT, "cores": cb["threads"], "kind": "reference",
                "sample": cb["sample"]}
+        if sub is not None:
+            sub["cpu_ms"] = cb["seconds"][0] * 1e3
+            sub["cpu_samples_per_s"] = v
+            sub["fp64_gpu_vs_cpu"] = sub["fp64_samples_per_s"] / v
+            sub["fp32c_gpu_vs_cpu"] = sub["fp32c_samples_per_s"] / v
 
     if rank == 0:
         line = {
@@ -690,17 +806,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "strong" if shard else "weak", "vs_baseline": None, "dtype": "f32c",
             "data": "synthetic",
-            "config": {"workload": f"{args.workload}: Nside "
-                       f"{'/'.join(str(s) for s in wl['nside_shells'])} x "
-                       f"{len(wl['nside_shells'])} shells to {wl['r_max_kpc']:g} kpc, "
-                       f"{wl['res_kpc']} kpc steps, {n}^3 FP32 grids, "
-                       f"{'/'.join(str(f) for f in wl['freqs_ghz'])} GHz",
-                       "samples_per_step": samples_step, "passes_per_step": len(passes),
-                       "l2": "inputs larger than L2 (grids "
-                             f"{4 * 4 * n ** 3 / 1e9:.2f} GB FP32)",
-                       "parallelism": (f"shell pixels split over {ws} GPUs, FD all-reduce "
-                                       "per shell" if shard else
-                                       f"replicas x{ws}" if ws > 1 else "1 GPU")},
+            "config": config_of(args, wl, ws, shard),
             "ms_per_map": ms_step / len(passes),
             "fp64": fp64,
             "fp32c_passes_one_by_one": one_by_one,
@@ -718,6 +824,9 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "e2e_fp64": e2e64,
+            # the bounded sample of cpu_baseline, timed in both GPU forms
+            "bounded_sample": sub,
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }

@@ -231,3 +231,96 @@ def samples_of(obs):
         step = int(math.floor(de / dd - ds / dd))
         tot += abi.npix(obs.nside_shell[s]) * step
     return tot
+
+
+# ---- samples that pass the cuts ----------------------------------------------
+
+def ring_directions(nside, start, stop):
+    """Unit vectors (x, y, z) of RING pixels [start, stop) of an Nside map:
+    the HEALPix pixel centres (Gorski et al. 2005, ApJ 622, 759, eqs. 4-9),
+    as Hampix::fillpoint computes them (include/hamdis.h:302-356)."""
+    p = np.arange(start, stop, dtype=np.int64)
+    n = int(nside)
+    npix, ncap = 12 * n * n, 2 * n * (n - 1)
+    z = np.empty(p.shape)
+    phi = np.empty(p.shape)
+    north = p < ncap
+    south = p >= npix - ncap
+    eq = ~(north | south)
+    if north.any():
+        q = p[north]
+        ir = np.floor(0.5 * (1.0 + np.sqrt(1.0 + 2.0 * q))).astype(np.int64)
+        iphi = q + 1 - 2 * ir * (ir - 1)
+        z[north] = 1.0 - ir * ir / (3.0 * n * n)
+        phi[north] = (iphi - 0.5) * (0.5 * math.pi / ir)
+    if eq.any():
+        q = p[eq] - ncap
+        ir = q // (4 * n) + n
+        iphi = q % (4 * n) + 1
+        fodd = 0.5 * (1 + ((ir + n) & 1))
+        z[eq] = (2 * n - ir) * (2.0 / (3.0 * n))
+        phi[eq] = (iphi - fodd) * (0.5 * math.pi / n)
+    if south.any():
+        q = npix - p[south]
+        ir = np.floor(0.5 * (1.0 + np.sqrt(2.0 * q - 1.0))).astype(np.int64)
+        iphi = 4 * ir + 1 - (q - 2 * ir * (ir - 1))
+        z[south] = -1.0 + ir * ir / (3.0 * n * n)
+        phi[south] = (iphi - 0.5) * (0.5 * math.pi / ir)
+    s = np.sqrt(np.maximum(0.0, (1.0 - z) * (1.0 + z)))
+    return s * np.cos(phi), s * np.sin(phi), z
+
+
+def _count_in(ds, dd, step, a, b):
+    """Number of sample indices i in [0, step) with ds + (i + 1/2) dd in
+    [a, b] (elementwise; empty where a > b)."""
+    lo = np.ceil((a - ds) / dd - 0.5)
+    hi = np.floor((b - ds) / dd - 0.5)
+    lo = np.clip(lo, 0, step)
+    hi = np.clip(hi, -1, step - 1)
+    return np.maximum(hi - lo + 1, 0).astype(np.int64)
+
+
+def valid_samples(obs, chunk=1 << 20):
+    """Per shell, the number of LOS samples that pass the galacto-centric
+    cuts gc_r_min <= |pos| <= gc_r_max and gc_z_min <= z <= gc_z_max
+    (integrator.cc:176-185): the samples whose fields are read and summed,
+    as opposed to the reference's loop count (samples_of).  Exact up to
+    samples within rounding of a cut boundary."""
+    o = np.array([obs.observer[i] for i in range(3)])
+    oo = float(o @ o)
+    out = []
+    for s in range(obs.total_shell):
+        d0, d1, res = obs.radii_shell[s], obs.radii_shell[s + 1], obs.oc_r_res
+        step = int(math.floor(d1 / res - d0 / res))      # assemble_shell_ref
+        dd = (d1 - d0) / step
+        nside = obs.nside_shell[s]
+        total = 0
+        for a in range(0, abi.npix(nside), chunk):
+            ux, uy, uz = ring_directions(nside, a, min(a + chunk, abi.npix(nside)))
+            ou = o[0] * ux + o[1] * uy + o[2] * uz
+            # |o + u d|^2 = d^2 + 2 (o.u) d + |o|^2 between r_min^2 and r_max^2
+            def roots(r):
+                disc = ou * ou - (oo - r * r)
+                sq = np.sqrt(np.maximum(disc, 0.0))
+                return -ou - sq, -ou + sq, disc >= 0.0
+            olo, ohi, _ = roots(obs.gc_r_max)
+            # z = o_z + u_z d in [z_min, z_max]
+            with np.errstate(divide="ignore", invalid="ignore"):
+                za = (obs.gc_z_min - o[2]) / uz
+                zb = (obs.gc_z_max - o[2]) / uz
+            zlo = np.where(uz != 0.0, np.minimum(za, zb), -np.inf)
+            zhi = np.where(uz != 0.0, np.maximum(za, zb), np.inf)
+            inside_z = (o[2] >= obs.gc_z_min) & (o[2] <= obs.gc_z_max)
+            zlo = np.where((uz == 0.0) & ~inside_z, np.inf, zlo)
+            lo, hi = np.maximum(olo, zlo), np.minimum(ohi, zhi)
+            n_out = _count_in(d0, dd, step, lo, hi)
+            if obs.gc_r_min > 0.0:
+                ilo, ihi, hit = roots(obs.gc_r_min)
+                # strictly inside the inner sphere: excluded
+                ilo, ihi = np.maximum(ilo, lo), np.minimum(ihi, hi)
+                n_in = _count_in(d0, dd, step, np.nextafter(ilo, np.inf),
+                                 np.nextafter(ihi, -np.inf))
+                n_out = n_out - np.where(hit, n_in, 0)
+            total += int(n_out.sum())
+        out.append(total)
+    return out

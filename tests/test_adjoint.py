@@ -125,3 +125,95 @@ def test_adjoint_cost_and_state_errors():
     with pytest.raises(_lib.HxgError) as e:
         integ.adjoint_device(maps.obs)     # no checkpointed forward yet
     assert e.value.status == abi.HXG_ERR_STATE
+
+
+@pytest.mark.slow
+def test_adjoint_config4_full_size():
+    """Config 4 as stated: 256^3 B (Grid_brnd) and n_e (Grid_ternd) grids
+    of the seeded synthetic fields, Nside 64/128/256 over 3 shells to 30 kpc
+    at 0.01 kpc, one 23 GHz pass with DM and FD; loss = sum over I, Q, U and
+    FD of ((map - target) / sigma)^2 with the target made from the 8
+    parameters perturbed by 1 % plus Gaussian noise of sigma = 1 % of each
+    map's maximum (seed 5).  The adjoint gradient is checked against central
+    differences (step 1e-4 relative, Richardson-extrapolated) for all 8
+    parameters and 32 voxels drawn with seed 6 among those the rays reach
+    (nonzero gradient): 16 of B (the three components) and 16 of n_e.  The
+    difference of two losses is summed from the difference of their maps,
+    which is exactly zero on pixels the perturbation does not reach, so a
+    single voxel's effect is not lost in the rounding of the 3-million-pixel
+    sum."""
+    from hammurabix_b200.autograd import LOSMaps, params_of
+    dev = torch.device("cuda", 0)
+    n = 256
+    bx, by, bz, ne = W.random_grids_torch(n, 1, 2, device=dev)
+    b = [t.double().reshape(-1).contiguous() for t in (bx, by, bz)]
+    dne = (ne.double().reshape(-1) - 0.03).contiguous()   # fluctuation on the disk
+    del bx, by, bz, ne
+    base = W.spiral_models()
+    base.tereg = abi.HXG_TEREG_EXPDISK
+    obs = W.make_obs([64, 128, 256], 30.0, 0.01, freq_ghz=23.0)
+    maps = LOSMaps(obs, base, W.grid_desc(n))
+    p0 = torch.tensor(params_of(maps.base), dtype=torch.float64, device=dev)
+    keep = (1, 2, 3, 4)          # FD, I, Q, U (dm, fd, is, qs, us order)
+    gen = torch.Generator(device=dev).manual_seed(5)
+    with torch.no_grad():
+        sign = torch.tensor([1, -1, 1, 1, -1, 1, -1, 1], dtype=torch.float64, device=dev)
+        outs = maps(p0 * (1.0 + 0.01 * sign), b, dne)
+        sig = {k: 0.01 * outs[k].abs().max().item() for k in keep}
+        target = {k: outs[k] + sig[k] * torch.randn(outs[k].shape, generator=gen,
+                                                     dtype=torch.float64, device=dev)
+                  for k in keep}
+
+    def loss_of(o):
+        return sum((((o[k] - target[k]) / sig[k]) ** 2).sum() for k in keep)
+
+    def dloss(op, om):
+        """loss(op) - loss(om) from the map differences."""
+        return sum(((op[k] - om[k]) * (op[k] + om[k] - 2.0 * target[k])).sum().item()
+                   / sig[k] ** 2 for k in keep)
+
+    p = p0.clone().requires_grad_(True)
+    bb = [t.clone().requires_grad_(True) for t in b]
+    nn = dne.clone().requires_grad_(True)
+    L = loss_of(maps(p, bb, nn))
+    L.backward()
+
+    def fwd(pv, bv, nv):
+        with torch.no_grad():
+            return [t.clone() for t in maps(pv, bv, nv)]
+
+    def richardson(make, h):
+        def cd(s):
+            return dloss(make(s), make(-s)) / (2.0 * s)
+        return (4.0 * cd(0.5 * h) - cd(h)) / 3.0
+
+    gp = p.grad.cpu().numpy()
+    for k in range(8):
+        h = 1e-4 * abs(p0[k].item())
+
+        def make(s, k=k):
+            q = p0.clone()
+            q[k] += s
+            return fwd(q, b, dne)
+        fd = richardson(make, h)
+        assert abs(gp[k] - fd) <= 2e-4 * max(abs(fd), abs(gp[k])) + 1e-10 * abs(L.item()) / abs(
+            p0[k].item()), (k, gp[k], fd)
+    rng = np.random.Generator(np.random.PCG64(6))
+    grads = [t.grad for t in bb] + [nn.grad]
+    arrays = list(b) + [dne]
+    checked = 0
+    for comp, count in ((0, 6), (1, 5), (2, 5), (3, 16)):
+        g = grads[comp]
+        reach = torch.nonzero(g.abs() > 1e-6 * g.abs().max()).reshape(-1).cpu().numpy()
+        rms = arrays[comp].std().item()
+        for i in rng.choice(reach, size=count, replace=False):
+            def make(s, comp=comp, i=i):
+                a = [t.clone() for t in arrays]
+                a[comp][i] += s
+                return fwd(p0, a[:3], a[3])
+            fd = richardson(make, 1e-4 * rms)
+            an = g[i].item()
+            assert abs(an - fd) <= 2e-4 * max(abs(fd), abs(an)) + 1e-8 * g.abs().max().item(), \
+                (comp, int(i), an, fd)
+            checked += 1
+    assert checked == 32

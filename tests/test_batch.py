@@ -184,3 +184,64 @@ def test_batch_follows_new_grids_and_refuses_a_new_geometry(fields32):
             b.run()
         assert e.value.status == abi.HXG_ERR_STATE
         b.close()
+
+
+def test_batch_config5_shape_against_oracle(oracle):
+    """A config-5-shaped FP32C batch: 6 spiral parameter sets (b0, pitch,
+    disk height drawn as in config 5) x 3 frequencies = 18 entries, 1-3
+    shells of Nside 64/128/256 to 15-30 kpc at 0.01 kpc, one shared 64^3
+    grid, in one graph with the autotuned shape.  Three entries (one of
+    each shell count) are compared directly with the CPU oracle
+    (oracle/hxo.c, the reference's write_grid restated) at the FP32C bound,
+    and every entry with the per-pass loop."""
+    dev = torch.device("cuda", 0)
+    rng = np.random.Generator(np.random.PCG64(7))
+    n = 64
+    fields = W.random_grids(n, 5, 6)
+    grids = W.grids_dict(n, *fields)
+    ents, nsh_of = [], []
+    for nsh in (3, 1, 2, 3, 2, 1):
+        m = W.grid_models(W.spiral_models(b0_muG=rng.uniform(2, 8),
+                                          pitch_deg=rng.uniform(-40, -5),
+                                          hb_kpc=rng.uniform(0.5, 2)))
+        rmax = rng.uniform(15, 30)
+        for k, f in enumerate((30.0, 1.4, 0.408)):
+            ents.append((m, W.make_obs([64 * 2 ** s for s in range(nsh)], rmax, 0.01,
+                                       freq_ghz=f, do_dm=(k == 0), do_fd=(k == 0))))
+            nsh_of.append(nsh)
+    assert len(ents) >= 16
+    dgrids = {f: (d, [torch.tensor(a, device=dev) for a in comps])
+              for f, (d, comps) in grids.items()}
+    with I.Integrator("fp32c") as integ:
+        integ.set_models(ents[0][0])
+        for f, (d, comps) in dgrids.items():
+            integ.upload_grid_device(f, d, comps)
+        got = [_outs(o, dev) for _, o in ents]
+        b = integ.batch([(m, o, g) for (m, o), g in zip(ents, got)], tune=True)
+        b.run()
+        integ.sync()
+        b.close()
+        loop = []
+        for m, o in ents:
+            integ.set_models(m)
+            outs = _outs(o, dev)
+            integ.write_grid_device(o, outs["dm"], outs["fd"], outs["is"], outs["qs"], outs["us"])
+            loop.append(outs)
+        integ.sync()
+    for k, (r, g) in enumerate(zip(loop, got)):
+        for key, t in r.items():
+            if t is not None:
+                e = rel_err(g[key].cpu().numpy(), t.cpu().numpy())
+                assert e <= 1e-5, (k, key, e)
+    # one entry per shell count, the low frequency (strongest rotation) for
+    # two of them and the DM/FD pass for the third
+    picks = [nsh_of.index(1) + 2, nsh_of.index(2), nsh_of.index(3) + 2]
+    for k in picks:
+        m, o = ents[k]
+        ref = oracle.write_grid(o, m, grids)
+        for key in ("dm", "fd", "is", "qs", "us"):
+            if ref[key] is None:
+                continue
+            assert np.abs(ref[key]).max() > 0, (k, key)
+            e = rel_err(got[k][key].cpu().numpy(), ref[key])
+            assert e <= 1e-5, (k, nsh_of[k], key, e)
