@@ -500,12 +500,15 @@ def main():
         def reduce_sum(t):
             dist.all_reduce(t)
 
+        def reduce_root(t):
+            dist.reduce(t, dst=0)
+
     def step(ig, outs):
         """One config-3 step: the frequency passes in the Pipeline's order,
         fused into one traversal per shell where the form allows (FP32C)."""
         if shard:
             sharded.write_passes_sharded(ig, passes, [dict(zip(sharded.MAPS, m)) for m in outs],
-                                         shell_tmp, rank, ws, reduce_sum)
+                                         shell_tmp, rank, ws, reduce_sum, reduce_root)
         else:
             ig.write_grid_multi_device([(o, sel(o, m)) for o, m in zip(passes, outs)])
 

@@ -10,8 +10,11 @@ are summed over the ranks (an all-reduce of one map of 12 nside_shell^2
 doubles; the shards are disjoint, so the sum is the full map), and every rank
 merges the complete FD map into its FD output, which is then identical on
 all ranks.  The DM and Stokes maps are merged from each rank's partial shell
-maps (the merge is linear) and summed over the ranks once at the end.  Every
-rank issues the same collectives in the same order.
+maps (the merge is linear) and summed onto rank 0 once at the end of the
+pass (a reduce, not an all-reduce: no rank but the first needs them), so
+after a pass rank 0 holds every output map and the other ranks the FD map
+and their own partial DM / I / Q / U.  Every rank issues the same
+collectives in the same order.
 """
 from . import abi
 
@@ -32,7 +35,7 @@ def shell_maps_needed(obs):
     return r
 
 
-def write_grid_sharded(integ, obs, outs, tmp, rank, world, reduce_sum):
+def write_grid_sharded(integ, obs, outs, tmp, rank, world, reduce_sum, reduce_root=None):
     """One pass on this rank.
 
     integ: an Integrator; its device calls are ordered with the caller's
@@ -40,7 +43,11 @@ def write_grid_sharded(integ, obs, outs, tmp, rank, world, reduce_sum):
     it that stream with Integrator.set_stream saves the event waits);
     outs: dict of the pass outputs (device tensors, the requested ones);
     tmp: dict of shell-map buffers of 12 max(nside_shell)^2 doubles;
-    reduce_sum(t): in-place sum of t over the ranks, in stream order."""
+    reduce_sum(t): in-place sum of t over the ranks onto every rank, in
+    stream order (the per-shell FD map);
+    reduce_root(t): in-place sum of t over the ranks onto rank 0 (the DM
+    and Stokes outputs at the end of the pass); reduce_sum if None."""
+    reduce_root = reduce_root or reduce_sum
     req, need = requested(obs), shell_maps_needed(obs)
     for k in MAPS:
         if req[k]:
@@ -57,7 +64,7 @@ def write_grid_sharded(integ, obs, outs, tmp, rank, world, reduce_sum):
     if world > 1:
         for k in ("dm", "is", "qs", "us"):
             if req[k]:
-                reduce_sum(outs[k])
+                reduce_root(outs[k])
 
 
 def make_shell_maps(n, zeros):
@@ -68,7 +75,7 @@ def make_shell_maps(n, zeros):
             "iqu": [[zeros(n) for _ in range(3)] for _ in range(3)]}
 
 
-def _fused_group(integ, group, outs, tmp, rank, world, reduce_sum):
+def _fused_group(integ, group, outs, tmp, rank, world, reduce_sum, reduce_root):
     """2 or 3 passes sharing one traversal per shell (the library refuses a
     group it cannot fuse before any work, with HXG_ERR_UNSUPPORTED)."""
     reqs = [requested(o) for o in group]
@@ -97,15 +104,17 @@ def _fused_group(integ, group, outs, tmp, rank, world, reduce_sum):
         for f, r in enumerate(reqs):
             for k in ("dm", "is", "qs", "us"):
                 if r[k]:
-                    reduce_sum(outs[f][k])
+                    reduce_root(outs[f][k])
 
 
-def write_passes_sharded(integ, passes, outs, tmp, rank, world, reduce_sum):
+def write_passes_sharded(integ, passes, outs, tmp, rank, world, reduce_sum, reduce_root=None):
     """Several frequency passes (the Pipeline's order) on this rank: groups
     of up to three passes that the library can fuse share one traversal per
     shell (hxg_shell_integrate_multi_device); the others run one by one.
-    outs: one dict of MAPS per pass; tmp: make_shell_maps(...)."""
+    outs: one dict of MAPS per pass; tmp: make_shell_maps(...); reduce_sum,
+    reduce_root as in write_grid_sharded."""
     from ._lib import HxgError
+    reduce_root = reduce_root or reduce_sum
     single = {"dm": tmp["dm"], "fd": tmp["fd"], "is": tmp["iqu"][0][0],
               "qs": tmp["iqu"][0][1], "us": tmp["iqu"][0][2]}
     k = 0
@@ -116,7 +125,8 @@ def write_passes_sharded(integ, passes, outs, tmp, rank, world, reduce_sum):
             if len(group) < nf:
                 continue
             try:
-                _fused_group(integ, group, outs[k:k + nf], tmp, rank, world, reduce_sum)
+                _fused_group(integ, group, outs[k:k + nf], tmp, rank, world, reduce_sum,
+                             reduce_root)
             except HxgError as e:
                 if e.status != abi.HXG_ERR_UNSUPPORTED:
                     raise
@@ -125,5 +135,6 @@ def write_passes_sharded(integ, passes, outs, tmp, rank, world, reduce_sum):
             done = True
             break
         if not done:
-            write_grid_sharded(integ, passes[k], outs[k], single, rank, world, reduce_sum)
+            write_grid_sharded(integ, passes[k], outs[k], single, rank, world, reduce_sum,
+                               reduce_root)
             k += 1

@@ -79,12 +79,13 @@ def _obs():
     return W.make_obs([4, 8, 8], 20.0, 0.1, freq_ghz=1.4)
 
 
-def _run(world, rank, reduce_sum):
+def _run(world, rank, reduce_sum, reduce_root=None):
     o = _obs()
     out_n = abi.npix(8)
     outs = {k: torch.zeros(out_n, dtype=torch.float64) for k in sharded.MAPS}
     tmp = {k: torch.zeros(out_n, dtype=torch.float64) for k in sharded.MAPS}
-    sharded.write_grid_sharded(FakeIntegrator(), o, outs, tmp, rank, world, reduce_sum)
+    sharded.write_grid_sharded(FakeIntegrator(), o, outs, tmp, rank, world, reduce_sum,
+                               reduce_root)
     return {k: v.numpy().copy() for k, v in outs.items()}
 
 
@@ -92,13 +93,13 @@ def _passes():
     return W.frequency_passes(W.make_obs([4, 8, 8], 20.0, 0.1, freq_ghz=1.4), [0.408, 1.4, 30.0])
 
 
-def _run_passes(world, rank, reduce_sum):
+def _run_passes(world, rank, reduce_sum, reduce_root=None):
     ps = _passes()
     out_n = abi.npix(8)
     z = lambda n: torch.zeros(n, dtype=torch.float64)
     outs = [{k: z(out_n) for k in sharded.MAPS} for _ in ps]
     sharded.write_passes_sharded(FakeIntegrator(), ps, outs, sharded.make_shell_maps(out_n, z),
-                                 rank, world, reduce_sum)
+                                 rank, world, reduce_sum, reduce_root)
     return [{k: v.numpy().copy() for k, v in o.items()} for o in outs]
 
 
@@ -115,13 +116,17 @@ def _rank(rank, ws, port, q):
     from hammurabix_b200 import replicas
     w, r, _ = replicas.init("gloo", 60)
     red = lambda t: dist.all_reduce(t)
-    q.put((r, (_run(w, r, red), _run_passes(w, r, red))))
+    root = lambda t: dist.reduce(t, dst=0)
+    q.put((r, (_run(w, r, red, root), _run_passes(w, r, red, root))))
     replicas.finish(w)
 
 
 def test_two_gloo_ranks_reproduce_the_single_process_pass():
     """One pass (per-shell exchange) and three fused passes of the
-    Pipeline's order, on two ranks, against one process."""
+    Pipeline's order, on two ranks, against one process: rank 0 ends with
+    every map of the single process (the DM and Stokes maps reduced onto
+    it), every rank with the complete FD map, and rank 1's DM and Stokes
+    maps stay its own shard's partial maps (no all-reduce at the end)."""
     single = _run(1, 0, None)
     single_multi = _run_passes(1, 0, None)
     ctx = mp.get_context("spawn")
@@ -138,12 +143,19 @@ def test_two_gloo_ranks_reproduce_the_single_process_pass():
         one, multi = got[r]
         for k in sharded.MAPS:
             assert np.abs(single[k]).max() > 0, k
-            assert rel_err(one[k], single[k]) <= 1e-12, (r, k)
+            if r == 0 or k == "fd":
+                assert rel_err(one[k], single[k]) <= 1e-12, (r, k)
+            else:
+                assert rel_err(one[k], single[k]) > 1e-3, (r, k)
         for p, (a, b) in enumerate(zip(multi, single_multi)):
             for k in sharded.MAPS:
                 if sharded.requested(_passes()[p])[k]:
                     assert np.abs(b[k]).max() > 0, (p, k)
-                    assert rel_err(a[k], b[k]) <= 1e-12, (r, p, k)
+                    if r == 0 or k == "fd":
+                        assert rel_err(a[k], b[k]) <= 1e-12, (r, p, k)
+    # rank 1 keeps its own shard's part of DM / I / Q / U, a nonzero share
+    for k in ("dm", "is", "qs", "us"):
+        assert np.abs(got[1][0][k]).max() > 0, k
 
 
 def test_shards_partition_every_shell():
