@@ -708,6 +708,13 @@ int build_launch(hxg_handle *h, const hxg_models_t &m, const hxg_obs_t &o,
     F.sp_ihs = 1. / D.sp_hs;
     F.sp_sin = D.sp_sin;
     F.sp_cos = D.sp_cos;
+    const double sgn = D.sp_b0 < 0. ? -1. : 1.;
+    F.sp_crs_l = F.sp_crs + (D.sp_b0 != 0. ? std::log(std::fabs(D.sp_b0)) : 0.);
+    F.sp_sin_s = sgn * D.sp_sin;
+    F.sp_cos_s = sgn * D.sp_cos;
+    F.sp_sinf_s = float(F.sp_sin_s);
+    F.sp_cosf_s = float(F.sp_cos_s);
+    F.ex_ln0 = D.tex_n0 > 0. ? std::log(D.tex_n0) : 0.;
     F.ex_n0 = D.tex_n0;
     F.ex_irn = 1. / D.tex_rs;
     F.ex_ihn = 1. / D.tex_hs;
@@ -720,6 +727,9 @@ int build_launch(hxg_handle *h, const hxg_models_t &m, const hxg_obs_t &o,
     F.cre_ir0 = float(1. / D.cre_r0);
     F.cre_2iz0 = float(2. / D.cre_z0);
     F.cre_R0 = float(D.cre_R0);
+    F.cre_ir0_l2 = float(cgs::log2e / D.cre_r0);
+    F.cre_2iz0_l2 = float(2. * cgs::log2e / D.cre_z0);
+    F.cre_R0_l2 = float(2. + D.cre_R0 * cgs::log2e / D.cre_r0);
     F.pe = float(P.em_pe);
   } else {
     P.fd_fore = fdfore;
@@ -761,7 +771,8 @@ int validate_obs(hxg_handle *h, const hxg_obs_t *o) {
     double ds, dd;
     uint64_t st;
     shell_ref(*o, s, ds, dd, st);
-    if (st < 1 || st > (1ull << 40))
+    // the shell kernels index a ray's samples with 32-bit integers
+    if (st < 1 || st > (1ull << 30))
       return fail(h, HXG_ERR_INVALID, "shell %u has %llu radial steps", s,
                   (unsigned long long)st);
   }
@@ -792,6 +803,13 @@ int slot_prepare(hxg_handle *h, int field, const hxg_grid_desc_t *g, size_t *n_o
     return fail(h, HXG_ERR_INVALID, "CRE grid needs nE >= 2, E_min > 0, E_fact > 0");
   if (g->nx < 2 || g->ny < 2 || g->nz < 2)
     return fail(h, HXG_ERR_INVALID, "grid needs at least 2 vertices per axis");
+  // the FP32C kernels step grid coordinates in 64-bit fixed point with 44
+  // fraction bits
+  if (g->nx > (1u << 19) || g->ny > (1u << 19) || g->nz > (1u << 19))
+    return fail(h, HXG_ERR_INVALID, "grid has more than 2^19 vertices on an axis");
+  // and index voxel records with 32-bit integers
+  if ((uint64_t)g->nx * g->ny * g->nz > 0xFFFFFFFFull)
+    return fail(h, HXG_ERR_INVALID, "grid has more than 2^32 - 1 vertices");
   if (!(g->x_max > g->x_min) || !(g->y_max > g->y_min) || !(g->z_max > g->z_min))
     return fail(h, HXG_ERR_INVALID, "grid box has non-positive extent");
   const int ncomp = (field == HXG_FIELD_BREG || field == HXG_FIELD_BRND) ? 3 : 1;

@@ -16,6 +16,7 @@ namespace hxg {
 // ---- CGS constants: same expressions as include/hamunits.h:10-67 --------
 namespace cgs {
 constexpr double pi = 3.141592653589793238462643383279502884197;
+constexpr double log2e = 1.4426950408889634;  // log2(e)
 constexpr double halfpi = 1.570796326794896619231321691639751442099;
 constexpr double twothirds = 0.666666666666666666666666666666666666667;
 constexpr double twopi = 6.283185307179586476925286766559005768394;

@@ -25,12 +25,20 @@ struct FastModels {
   double sp_b0, sp_irs, sp_crs, sp_ihs;  // amplitude, 1/r_s, r_sun/r_s, 1/h_s
   double sp_sin, sp_cos;                 // sin, cos of the pitch angle
   double ex_n0, ex_irn, ex_ihn;          // exp-disk n0, 1/r_s, 1/h_s
+  // the kFast sample loop folds the amplitudes into the exponents:
+  // r_sun/r_s + ln|b0| and ln n0, the sign of b0 into sp_*_s
+  double sp_crs_l, ex_ln0;
+  double sp_sin_s, sp_cos_s;             // sign(b0) sin, sign(b0) cos
+  float sp_sinf_s, sp_cosf_s;            // the same in FP32
   // launch constants in the types the sample loop uses, so that the loop
   // reads them as operands instead of converting them
   double r2min, r2max;                   // gc_r_min^2, gc_r_max^2
   double rc2_hi, rc2_lo;                 // spiral cylinder: (20 kpc)^2, (3 kpc)^2
   float sp_sinf, sp_cosf;                // sp_sin, sp_cos
   float cre_ir0, cre_2iz0, cre_R0;       // CRE_ana: 1/r0, 2/z0, R0
+  // the same for base-2 exponentials: log2(e)/r0, 2 log2(e)/z0 and
+  // 2 + R0 log2(e)/r0 (the factor 4 of 4 e^x / (1 + t)^2 folded in)
+  float cre_ir0_l2, cre_2iz0_l2, cre_R0_l2;
   float pe;                              // em_pe
 };
 
@@ -80,13 +88,17 @@ struct ShellLaunch {
 };
 
 // The models of the grid workloads: B none, grid or spiral; n_e none, grid
-// or exponential disk; CRE_ana with a constant index.  The shell kernels
-// have an instantiation (kFast) for launches whose models are among these,
-// with the other models' paths compiled out, so that its registers are
-// allocated for this path alone.
+// or exponential disk; CRE_ana with a constant index; no inner radius cut
+// (gc_r_min = 0, so that the samples of a ray that pass the cuts are one
+// contiguous run).  The shell kernels have an instantiation (kFast) for
+// launches whose models are among these, with the other models' paths
+// compiled out, so that its registers are allocated for this path alone.
 __host__ __device__ inline bool fast_models(const ShellLaunch &P) {
   const DevModels &M = P.models;
-  return P.ext == nullptr &&
+  return P.ext == nullptr && !(P.gc_r_min > 0.) &&
+         // amplitudes folded into the exponents as logarithms (FastModels)
+         (M.breg != kBregSpiral || M.sp_b0 != 0.) &&
+         (M.tereg != kTeregExpdisk || M.tex_n0 > 0.) &&
          (M.breg == kBregNone || M.breg == kBregGrid || M.breg == kBregSpiral) &&
          (M.tereg == kTeregNone || M.tereg == kTeregGrid || M.tereg == kTeregExpdisk) &&
          (!P.do_sync || (M.cre == kCreAna && P.em_const));

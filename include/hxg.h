@@ -223,7 +223,9 @@ int hxg_set_models(hxg_handle *h, const hxg_models_t *m);
 /* ---- grids: the Grid_* SoA arrays (include/grid.h:63,94,117,144,167).
  * field = HXG_FIELD_*; c0,c1,c2 = bx,by,bz for B slots, c0 = te for n_e
  * slots, c0 = cre_flux for the CRE slot (c1,c2 ignored).  Host FP64; the
- * library keeps its own device copy (FP64 and/or FP32 per precision).     */
+ * library keeps its own device copy (FP64 and/or FP32 per precision).
+ * 2 to 2^19 vertices per axis and at most 2^32 - 1 in all
+ * (HXG_ERR_INVALID otherwise).                                            */
 int hxg_upload_grid(hxg_handle *h, int field, const hxg_grid_desc_t *g,
                     const double *c0, const double *c1, const double *c2);
 /* Load a grid straight from the reference's binary grid file
@@ -286,7 +288,8 @@ int hxg_set_mask(hxg_handle *h, uint32_t nside, const double *mask);
  * Outputs are the Grid_obs maps after the shell loop, before
  * Grid_obs::export_grid's unit rescale: dm at nside_dm, fd at nside_fd,
  * is/qs/us at nside_sync.  Pointers for observables not requested by obs
- * may be NULL.  Host buffers; the call synchronises its stream.           */
+ * may be NULL.  Host buffers; the call synchronises its stream.  A shell
+ * may have up to 2^30 radial steps (HXG_ERR_INVALID beyond).              */
 int hxg_write_grid(hxg_handle *h, const hxg_obs_t *obs, double *dm,
                    double *fd, double *is, double *qs, double *us);
 /* Same with device output buffers; asynchronous on the handle's stream.   */
