@@ -361,7 +361,7 @@ def batch_config5(args, dev, stream, torch):
     del bx, by, bz, ne
     rng = np.random.Generator(np.random.PCG64(7))
     entries = []
-    for _ in range(256):
+    for _ in range(args.batch_sets):
         m = W.grid_models(W.spiral_models(b0_muG=rng.uniform(2, 8), pitch_deg=rng.uniform(-40, -5),
                                           hb_kpc=rng.uniform(0.5, 2)))
         nsh = int(rng.integers(1, 4))
@@ -402,7 +402,7 @@ def batch_config5(args, dev, stream, torch):
     b.close()
     ig.close()
     S = info["samples"]
-    return {"workload": "config5: 256 spiral parameter sets x 3 frequencies, 1-3 shells of "
+    return {"workload": f"config5: {args.batch_sets} spiral parameter sets x 3 frequencies, 1-3 shells of "
                         "Nside 64/128/256 to 15-30 kpc, 0.01 kpc steps, 256^3 FP32 grid, FP32C",
             "passes": len(entries), "samples": S, "batch_ms": batch_ms, "loop_ms": loop_ms,
             "batch_samples_per_s": S / (batch_ms / 1e3), "loop_samples_per_s": S / (loop_ms / 1e3),
@@ -430,6 +430,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--adjoint-steps", type=int, default=2)
     ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--batch-sets", type=int, default=256,
+                    help="parameter sets of the config-5 batch (256 in config 5)")
     ap.add_argument("--rfg-steps", type=int, default=2)
     ap.add_argument("--rfg-grid", type=int, default=WORKLOADS["config3"]["grid_n"],
                     help="cells per axis of the generator timing grid")
