@@ -277,11 +277,11 @@ def generators(args, dev, stream, torch):
     return res
 
 
-def adjoint_ratio(args, dev, stream, torch):
+def adjoint_ratio(args, dev, stream, torch, prec="fp64"):
     """Adjoint vs forward device time on the config-4 workload: Nside
     64/128/256 over 3 shells to 30 kpc, 256^3 grids (B read as Grid_brnd,
     n_e fluctuations as Grid_ternd on the exponential disk), spiral B, CRE_ana,
-    one 23 GHz pass with DM and FD; FP64 form with per-shell checkpointing.
+    one 23 GHz pass with DM and FD; form `prec` with per-shell checkpointing.
     The adjoint produces dL/d(8 parameters) and dL/d(every B and n_e voxel)."""
     from hammurabix_b200 import abi, workloads as W
     from hammurabix_b200.integrator import Integrator
@@ -296,7 +296,7 @@ def adjoint_ratio(args, dev, stream, torch):
     m.tereg = abi.HXG_TEREG_EXPDISK
     m.ternd = abi.HXG_TERND_GRID
     o = W.make_obs([64, 128, 256], 30.0, 0.01, freq_ghz=23.0)
-    ig = Integrator("fp64")
+    ig = Integrator(prec)
     ig.set_stream(stream.cuda_stream)
     ig.set_models(m)
     ig.upload_grid_device(abi.HXG_FIELD_BRND, desc, grids)
@@ -335,8 +335,8 @@ def adjoint_ratio(args, dev, stream, torch):
             plain.append(ev[0].elapsed_time(ev[1]))
     ig.close()
     f, a, fp = sum(fwd) / len(fwd), sum(adj) / len(adj), sum(plain) / len(plain)
-    return {"workload": "config4: Nside 64/128/256 x 3 shells to 30 kpc, 256^3 FP64 grids, "
-                        "23 GHz + DM + FD, FP64 form",
+    return {"workload": "config4: Nside 64/128/256 x 3 shells to 30 kpc, 256^3 grids, "
+                        f"23 GHz + DM + FD, {prec.upper()} form",
             "forward_ms": f, "adjoint_ms": a, "ratio": a / f,
             "forward_plain_ms": fp, "ratio_vs_plain_forward": a / fp,
             "checkpoint_overhead": f / fp - 1.0,
@@ -729,10 +729,12 @@ def main():
     e2e64 = e2e_leg("fp64", args.e2e64_steps) if args.e2e64_steps > 0 else None
 
     # ---- adjoint / forward cost on the config-4 workload (FP64 form) -------
-    adjoint = None
+    adjoint = adjoint64 = None
     if args.adjoint_steps > 0:
-        adjoint = adjoint_ratio(args, dev, stream, torch)
-        log(f"[rank {rank}] adjoint: {adjoint}")
+        # the product form's adjoint, and the parity form's
+        adjoint = adjoint_ratio(args, dev, stream, torch, "fp32c")
+        adjoint64 = adjoint_ratio(args, dev, stream, torch, "fp64")
+        log(f"[rank {rank}] adjoint: {adjoint} {adjoint64}")
 
     # ---- config-5 batch: one graph vs a per-pass loop --------------------------
     batch = None
@@ -824,6 +826,7 @@ def main():
             "fp32c_max_rel_err_vs_fp64": errs,
             "adjoint_fwd_ratio": adjoint["ratio"] if adjoint else None,
             "adjoint": adjoint,
+            "adjoint_fp64": adjoint64,
             "batch": batch,
             "generators": rfg,
             "roofline": roofline,

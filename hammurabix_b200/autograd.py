@@ -1,4 +1,4 @@
-"""PyTorch autograd for the line-of-sight integrator (FP64 form).
+"""PyTorch autograd for the line-of-sight integrator (FP64 or FP32C form).
 
 ``LOSMaps`` maps differentiable inputs -- the 8 regular-field parameters
 (spiral B: b0, pitch, r_scale, h_scale; exponential n_e disk: n0, r_scale,
@@ -75,16 +75,20 @@ class _LOSFunction(torch.autograd.Function):
 
 
 class LOSMaps:
-    """Differentiable forward map of one frequency pass (FP64 form)."""
+    """Differentiable forward map of one frequency pass.  precision "fp64"
+    (the parity form, every model) or "fp32c" (the FP32-compensated forward
+    and its adjoint: the grid workloads' models -- spiral B, exponential n_e
+    disk, CRE_ana with a constant index -- on one grid geometry)."""
 
-    def __init__(self, obs, base_models, grid_desc, device=0):
+    def __init__(self, obs, base_models, grid_desc, device=0, precision="fp64"):
         self.obs = obs
         self.base = abi.Models.from_buffer_copy(base_models)
         self.base.brnd = abi.HXG_BRND_GRID
         self.base.ternd = abi.HXG_TERND_GRID
         self.desc = grid_desc
         self.device = torch.device("cuda", device)
-        self.integ = Integrator("fp64", device=device)
+        self.precision = precision
+        self.integ = Integrator(precision, device=device)
         self.integ.set_checkpointing(True)
 
     def new_outputs(self):

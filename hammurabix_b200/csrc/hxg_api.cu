@@ -22,6 +22,7 @@
 
 #include "../../include/hxg.h"
 #include "hxg_adjoint.cuh"
+#include "hxg_adjoint32.cuh"
 #include "hxg_batch.cuh"
 #include "hxg_integrate.cuh"
 #include "hxg_internal.h"
@@ -1443,7 +1444,7 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
   }
   const ExtModels *ext_dev = nullptr;
   if ((st = upload_ext(h, h->models, o->sync_freq, &ext_dev)) != HXG_OK) return st;
-  const bool ck = h->checkpoint && !fp32;
+  const bool ck = h->checkpoint;
   for (uint32_t s = 0; s < o->total_shell; ++s) {
     st = run_shell(h, *o, s, ext_dev, d_fd, tmp, 0, 1, ck);
     if (st != HXG_OK) return st;
@@ -1796,8 +1797,6 @@ int hxg_shell_merge_device(hxg_handle *h, const hxg_obs_t *o, uint32_t shell,
 
 int hxg_set_checkpointing(hxg_handle *h, int enable) {
   if (!h) return HXG_ERR_INVALID;
-  if (enable && h->precision != HXG_FP64)
-    return fail(h, HXG_ERR_UNSUPPORTED, "the adjoint runs on the FP64 form only");
   h->checkpoint = enable != 0;
   h->ck_valid = false;
   return HXG_OK;
@@ -1814,6 +1813,7 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
                        double *d_grad_ne) {
   if (!h || !o) return HXG_ERR_INVALID;
   cudaSetDevice(h->device);
+  const bool fp32 = h->precision == HXG_FP32C;
   if (!h->ck_valid || std::memcmp(&h->ck_obs, o, sizeof(*o)) != 0 ||
       std::memcmp(&h->ck_models, &h->models, sizeof(h->models)) != 0)
     return fail(h, HXG_ERR_STATE,
@@ -1883,6 +1883,11 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
     const int C = h->ck_chunks[s];
     F.chunks = C;
     F.log2_chunks = hpx_ilog2((uint64_t)C);
+    if (fp32 && !fast_models(F))
+      return fail(h, HXG_ERR_UNSUPPORTED,
+                  "the FP32C adjoint covers the grid workloads' models (spiral or no regular "
+                  "B, exponential disk or no regular n_e, CRE_ana with a constant index, no "
+                  "inner radius cut); run the FP64 form");
     AdjointLaunch A{};
     A.F = F;
     A.ck = static_cast<const double *>(h->ck[s].p);
@@ -1893,9 +1898,10 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
     A.g_fdmap = gfdmap;
     A.want_j0 = (h->models.cre == HXG_CRE_ANA || h->models.cre == HXG_CRE_UNIF) ? 1 : 0;
     const uint64_t warps = (npix + (32 / C) - 1) / (32 / C);
-    const unsigned threads = HXG_ADJ_THREADS;
+    const unsigned threads = fp32 ? HXG_ADJ32_THREADS : HXG_ADJ_THREADS;
     const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
-    HXG_CK(launch_adjoint(h->stream, A, blocks, threads));
+    HXG_CK(fp32 ? launch_adjoint32(h->stream, A, blocks, threads)
+                : launch_adjoint(h->stream, A, blocks, threads));
     ++h->launch_count;
   }
   // parameter gradients: j0 slot holds sum (dL/dJ) J, divide by j0
@@ -1905,6 +1911,15 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
   const double j0 = h->models.cre == HXG_CRE_ANA ? h->models.cre_ana.j0
                                                  : h->models.cre_unif.j0;
   gp[7] = (j0 != 0.) ? gp[7] / j0 : 0.;
+  if (fp32) {
+    // the FP32C kernel sums log-derivatives for the amplitudes and
+    // per-kpc derivatives for the lengths (hxg_adjoint32.cuh)
+    const auto &sp = h->models.spiral;
+    const auto &ex = h->models.te_exp;
+    gp[0] = sp.b0 != 0. ? gp[0] / sp.b0 : 0.;
+    gp[4] = ex.n0 != 0. ? gp[4] / ex.n0 : 0.;
+    for (int k : {2, 3, 5, 6}) gp[k] /= cgs::kpc;
+  }
   if (d_grad_params)
     HXG_CK(cudaMemcpyAsync(d_grad_params, gp, sizeof(gp), cudaMemcpyHostToDevice, h->stream));
   if (ngrid && (d_grad_bx || d_grad_ne)) {
@@ -1912,7 +1927,8 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
     const bool has_b = G.b_slots[0] >= 0, has_t = G.t_slots[0] >= 0;
     HXG_CK(launch_unpack_grad(h->stream, ngrid, static_cast<const double *>(h->grad_rec.p),
                               has_b ? d_grad_bx : nullptr, has_b ? d_grad_by : nullptr,
-                              has_b ? d_grad_bz : nullptr, has_t ? d_grad_ne : nullptr));
+                              has_b ? d_grad_bz : nullptr, has_t ? d_grad_ne : nullptr,
+                              fp32 ? 1.0 / cgs::fp32_bunit : 1.0));
   }
   HXG_CK(cudaStreamSynchronize(h->stream));
   return HXG_OK;

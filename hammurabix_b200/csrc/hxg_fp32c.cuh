@@ -248,6 +248,15 @@ __device__ __forceinline__ float ex2_approx(float x) {
   return y;
 }
 
+// CRE_ana spatial profile exp((R0 - r)/r0) sech^2(z/z0) (cre_ana.cc:11-63)
+// in FP32 at cylindrical radius rf and height zf (kpc):
+//   = 2^(2 + (R0 - r) log2(e)/r0) t / (1 + t)^2, t = 2^(-2|z| log2(e)/z0).
+__device__ __forceinline__ float cre_ana_prof32(const FastModels &F, float rf, float zf) {
+  const float t = ex2_approx(-fabsf(zf) * F.cre_2iz0_l2);
+  const float den = 1.f + t;
+  return __fdividef(ex2_approx(fmaf(-rf, F.cre_ir0_l2, F.cre_R0_l2)) * t, den * den);
+}
+
 template <int NF>
 __device__ __forceinline__ void combine_chunks_nf(const ShellLaunch &P, const FreqSet<NF> &Fq,
                                                   int c, double &dm, double &fd, double si[NF],
@@ -318,6 +327,7 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
       const Hpx hf = hpx_make((uint64_t)P.nside_fdmap);
       inner = hpx_interpolate(hf, P.fdmap, th, ph);
     }
+    if (NF == 1 && P.ck_inner != nullptr && c == 0) P.ck_inner[ring] = inner;
     const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
     const double ux = cp * st, uy = sp * st, uz = ct;
     const float etx = float(ct * cp), ety = float(ct * sp), etz = float(-st);
@@ -533,9 +543,7 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
               const float r2f = fmaf(xf, xf, yf * yf);
               rf = r2f * rsqrtf(fmaxf(r2f, 1e-30f));
             }
-            const float t = ex2_approx(-fabsf(zf) * F.cre_2iz0_l2);
-            const float den = 1.f + t;
-            prof = __fdividef(ex2_approx(fmaf(-rf, F.cre_ir0_l2, F.cre_R0_l2)) * t, den * den);
+            prof = cre_ana_prof32(F, rf, zf);
           } else {
             prof = cre_profile<float>(M, xf, yf, zf, p3);
           }
@@ -619,6 +627,14 @@ __device__ __forceinline__ void fp32c_tile(const ShellLaunch &P, const FreqSet<N
       sq[f] = kq[f].value() * Fq.k_p[f];
       su[f] = ku[f].value() * Fq.k_p[f];
     }
+  }
+  // adjoint checkpoint (one pass): the chunk's FD and local-frame Q, U
+  // before the chunk combination, in the FP64 form's units
+  if (NF == 1 && P.ck != nullptr && live) {
+    const unsigned long long ci = nest * (unsigned long long)C + c;
+    P.ck[3 * ci] = fd;
+    P.ck[3 * ci + 1] = sq[0];
+    P.ck[3 * ci + 2] = su[0];
   }
   combine_chunks_nf<NF>(P, Fq, c, dm, fd, si, sq, su);
   if (live && c == 0) {

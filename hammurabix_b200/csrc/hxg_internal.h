@@ -57,6 +57,9 @@ cudaError_t launch_accumulate_transpose(cudaStream_t s, int nside_out,
                                         double *g_shell, double scale);
 cudaError_t launch_adjoint(cudaStream_t s, const AdjointLaunch &A,
                            unsigned blocks, unsigned threads);
+// The FP32C form's adjoint (the grid workloads' models, at most one grid).
+cudaError_t launch_adjoint32(cudaStream_t s, const AdjointLaunch &A, unsigned blocks,
+                             unsigned threads);
 // fast: every plan's models satisfy fast_models (the kFast instantiations).
 cudaError_t launch_batch_level(cudaStream_t s, bool fp32, int ngroups, bool ext, bool fast,
                                const BatchLevel &B, unsigned blocks);
@@ -79,7 +82,7 @@ cudaError_t launch_interleave3(cudaStream_t s, uint64_t n, const double *x, cons
                                const double *z, double *dst);
 cudaError_t launch_unpack_grad(cudaStream_t s, uint64_t n, const double *rec,
                                double *gbx, double *gby, double *gbz,
-                               double *gne);
+                               double *gne, double bscale);
 
 // Random-field generators (hxg_rfg.cu); synchronous on s, HXG_* status.
 // `work` is the caller's workspace (created on first use, kept for the next

@@ -5,6 +5,7 @@
 #include <type_traits>
 
 #include "hxg_adjoint.cuh"
+#include "hxg_adjoint32.cuh"
 #include "hxg_batch.cuh"
 #include "hxg_fp32c.cuh"
 #include "hxg_integrate.cuh"
@@ -160,14 +161,17 @@ __global__ void accumulate_transpose_kernel(int nside_out, int nside_shell,
 }
 
 // Split the group-record gradient [N][4] into B (3 SoA arrays) and n_e.
+// Record gradient -> per-slot gradients; bscale converts the B gradient
+// from the records' field unit to the slots' (1 in the FP64 form, 2^20 per
+// Gauss in the FP32C form, whose records hold B in 2^-20 G).
 __global__ void unpack_grad_kernel(uint64_t n, const double *rec, double *gbx,
-                                   double *gby, double *gbz, double *gne) {
+                                   double *gby, double *gbz, double *gne, double bscale) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (gbx) {
-    gbx[i] = rec[4 * i];
-    gby[i] = rec[4 * i + 1];
-    gbz[i] = rec[4 * i + 2];
+    gbx[i] = rec[4 * i] * bscale;
+    gby[i] = rec[4 * i + 1] * bscale;
+    gbz[i] = rec[4 * i + 2] * bscale;
   }
   if (gne) gne[i] = rec[4 * i + 3];
 }
@@ -498,10 +502,19 @@ cudaError_t launch_adjoint(cudaStream_t s, const AdjointLaunch &A,
   return cudaGetLastError();
 }
 
+cudaError_t launch_adjoint32(cudaStream_t s, const AdjointLaunch &A, unsigned blocks,
+                             unsigned threads) {
+  if (A.F.ngroups == 0)
+    shell_fp32c_adjoint_kernel<0><<<blocks, threads, 0, s>>>(A);
+  else
+    shell_fp32c_adjoint_kernel<1><<<blocks, threads, 0, s>>>(A);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_unpack_grad(cudaStream_t s, uint64_t n, const double *rec,
                                double *gbx, double *gby, double *gbz,
-                               double *gne) {
-  unpack_grad_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, rec, gbx, gby, gbz, gne);
+                               double *gne, double bscale) {
+  unpack_grad_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, rec, gbx, gby, gbz, gne, bscale);
   return cudaGetLastError();
 }
 

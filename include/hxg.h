@@ -362,10 +362,16 @@ int hxg_shell_merge_device(hxg_handle *h, const hxg_obs_t *obs, uint32_t shell,
                            double *d_is, double *d_qs, double *d_us);
 
 /* ---- adjoint (gradients of a scalar loss of the maps) -------------------
- * Reverse mode of hxg_write_grid_device (FP64 form).  With checkpointing
- * on, every forward call stores per shell the chunk Faraday depths and
- * Q, U partial sums and the inner-shell Faraday depth of each pixel; the
- * adjoint then runs one backward sweep per shell, outer shells first.
+ * Reverse mode of hxg_write_grid_device, in the handle's form.  With
+ * checkpointing on, every forward call stores per shell the chunk Faraday
+ * depths and Q, U partial sums and the inner-shell Faraday depth of each
+ * pixel; the adjoint then runs one backward sweep per shell, outer shells
+ * first.  The FP64 form covers every model the forward does except the
+ * CRE grid; the FP32C form (FP32 fields and emissivity, FP64 Faraday path,
+ * agreeing with the FP64 gradient to about 1e-5) covers the grid
+ * workloads' models -- spiral or no regular B, exponential disk or no
+ * regular n_e, CRE_ana with a constant index, gc_r_min = 0 -- and returns
+ * HXG_ERR_UNSUPPORTED for others.
  *
  * Inputs: dL/d(output maps) on the device (same sizes as the forward's
  * outputs; NULL = zero).  Outputs (device, overwritten, NULL = skip):
