@@ -45,9 +45,11 @@ WORKLOADS = {
                     freqs_ghz=[0.408, 1.4, 30.0], grid_n=256, seeds=(3, 4)),
 }
 # The bounded sample both arms time like for like: the first frequency pass
-# (DM + FD + synchrotron) of the workload over its two innermost shells
-# only, with their own radii, Nsides and sample positions, on the same grids.
-SUB_SHELLS = 2
+# (DM + FD + synchrotron) of the workload over its innermost shell only,
+# with its own radii, Nside and sample positions, on the same grids (config
+# 3: Nside 128, 0-3.75 kpc, 7.4e7 LOS samples, about 1.5 s of the
+# reference on 16 host threads per step).
+SUB_SHELLS = 1
 
 
 def log(*a):
@@ -167,8 +169,9 @@ def sub_workload_text(wl):
     from hammurabix_b200 import units as U
     o = sub_workload(wl)
     shells = "/".join(str(o.nside_shell[i]) for i in range(o.total_shell))
-    return (f"pass 1 ({o.sync_freq / 1e9:g} GHz with DM + FD) over the workload's {SUB_SHELLS} "
-            f"innermost shells (Nside {shells}, 0-{o.radii_shell[SUB_SHELLS] / U.kpc:g} kpc), "
+    what = "innermost shell" if SUB_SHELLS == 1 else f"{SUB_SHELLS} innermost shells"
+    return (f"pass 1 ({o.sync_freq / 1e9:g} GHz with DM + FD) over the workload's {what} "
+            f"(Nside {shells}, 0-{o.radii_shell[SUB_SHELLS] / U.kpc:g} kpc), "
             f"same {wl['grid_n']}^3 grids: {W.samples_of(o)} LOS samples, "
             f"Integrator::write_grid only")
 
