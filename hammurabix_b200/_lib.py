@@ -32,6 +32,7 @@ SIGNATURES = {
     "hxg_set_timing": (C.c_int, [_h, C.c_int]),
     "hxg_get_timing": (C.c_int, [_h, _dp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "hxg_get_launch_count": (C.c_int, [_h, C.POINTER(C.c_int64)]),
+    "hxg_set_interp_cache": (C.c_int, [_h, C.c_uint64]),
     "hxg_write_grid_noalloc": (C.c_int, [C.POINTER(abi.Obs), C.POINTER(abi.Models),
                                          C.POINTER(abi.GridDesc), _vp, _vp, _vp, _vp, _vp,
                                          _vp, _vp]),

@@ -74,6 +74,11 @@ struct hxg_handle {
   std::map<uint32_t, unsigned char *> mask_dev;
   DevBuf tmp[5];
   DevBuf tmp_multi[6];  // I/Q/U shell maps of the 2nd and 3rd fused pass
+  DevBuf shell_all;     // every shell's DM and Stokes maps of a pass
+  // interpolation tables by (output Nside << 32 | shell Nside)
+  std::map<uint64_t, DevBuf> interp;
+  size_t interp_bytes = 0;
+  size_t interp_limit = 8ull << 30;
   DevBuf out[5];
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -942,6 +947,8 @@ int hxg_destroy(hxg_handle *h) {
     if (b.p) cudaFree(b.p);
   for (auto &b : h->tmp_multi)
     if (b.p) cudaFree(b.p);
+  if (h->shell_all.p) cudaFree(h->shell_all.p);
+  for (auto &kv : h->interp) cudaFree(kv.second.p);
   for (auto &b : h->out)
     if (b.p) cudaFree(b.p);
   for (auto &b : h->ck)
@@ -1383,6 +1390,45 @@ int run_shell(hxg_handle *h, const hxg_obs_t &o, uint32_t s, const ExtModels *ex
   return HXG_OK;
 }
 
+// The interpolation table of an Nside pair, made on first use on the
+// handle's stream.  Null members (the kernels then find the weights in
+// place) when the Nsides agree, the shell map has more than 2^32 pixels,
+// the tables would pass the handle's bound (hxg_set_interp_cache) or the
+// allocation fails.
+int interp_tab(hxg_handle *h, uint32_t nside_dst, uint32_t nside_src, InterpTab *t) {
+  *t = InterpTab{};
+  if (nside_dst == nside_src || npix_of(nside_src) > 0xffffffffull) return HXG_OK;
+  const uint64_t key = (uint64_t)nside_dst << 32 | nside_src;
+  auto it = h->interp.find(key);
+  if (it == h->interp.end()) {
+    const size_t n = npix_of(nside_dst);
+    const size_t bytes = n * (sizeof(uint4) + 2 * sizeof(double2));
+    if (h->interp_bytes + bytes > h->interp_limit) return HXG_OK;
+    DevBuf b;
+    if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return HXG_OK;
+    }
+    b.bytes = bytes;
+    const cudaError_t e = launch_interp_table(h->stream, (int)nside_dst, (int)nside_src,
+                                              static_cast<uint4 *>(b.p),
+                                              reinterpret_cast<double2 *>(
+                                                  static_cast<char *>(b.p) + n * sizeof(uint4)));
+    if (e != cudaSuccess) {
+      cudaFree(b.p);
+      return cuda_fail(h, e, "launch_interp_table");
+    }
+    ++h->launch_count;
+    h->interp_bytes += bytes;
+    it = h->interp.emplace(key, b).first;
+  }
+  const size_t n = npix_of(nside_dst);
+  t->pix = static_cast<const uint4 *>(it->second.p);
+  t->w = reinterpret_cast<const double2 *>(static_cast<const char *>(it->second.p) +
+                                           n * sizeof(uint4));
+  return HXG_OK;
+}
+
 // Accumulate the shell maps of shell s into the pass outputs
 // (Hampix::accumulate, integrator.cc:121-132).
 int merge_shell(hxg_handle *h, const hxg_obs_t &o, uint32_t s, const double *const tmp[5],
@@ -1407,8 +1453,68 @@ int merge_shell(hxg_handle *h, const hxg_obs_t &o, uint32_t s, const double *con
         ++n;
         done[b] = true;
       }
-    HXG_CK(launch_accumulate(h->stream, (int)nside[a], ns, n, d, sr));
+    InterpTab tab;
+    int st = interp_tab(h, nside[a], (uint32_t)ns, &tab);
+    if (st != HXG_OK) return st;
+    HXG_CK(launch_accumulate(h->stream, (int)nside[a], ns, n, d, sr, &tab));
     ++h->launch_count;
+  }
+  return HXG_OK;
+}
+
+// One block of nm shell maps per shell in h->shell_all, for a pass whose DM
+// and Stokes maps are merged at its end: base[s] = shell s's block.
+int shell_blocks(hxg_handle *h, const hxg_obs_t &o, int nm, double **base) {
+  size_t off[HXG_MAX_SHELLS], total = 0;
+  for (uint32_t s = 0; s < o.total_shell; ++s) {
+    off[s] = total;
+    total += (size_t)nm * npix_of(o.nside_shell[s]);
+  }
+  const int st = ensure(h, h->shell_all, total * sizeof(double));
+  if (st != HXG_OK) return st;
+  for (uint32_t s = 0; s < o.total_shell; ++s)
+    base[s] = static_cast<double *>(h->shell_all.p) + off[s];
+  return HXG_OK;
+}
+
+// An output of the pass-end merge: the map idx of every shell's block summed
+// into dst at Nside nside.
+struct PassOut {
+  uint32_t nside;
+  int idx;
+  double *dst;
+};
+
+// The pass-end merge of the DM and Stokes maps (Hampix::accumulate of every
+// shell, integrator.cc:121-132, in shell order into the zeroed outputs): one
+// launch per output Nside.
+int merge_pass(hxg_handle *h, const hxg_obs_t &o, double *const *base,
+               const std::vector<PassOut> &outs) {
+  int nside[HXG_MAX_SHELLS];
+  const double *b[HXG_MAX_SHELLS];
+  InterpTab tab[HXG_MAX_SHELLS];
+  for (uint32_t s = 0; s < o.total_shell; ++s) {
+    nside[s] = (int)o.nside_shell[s];
+    b[s] = base[s];
+  }
+  std::vector<bool> done(outs.size(), false);
+  for (size_t a = 0; a < outs.size(); ++a) {
+    if (done[a]) continue;
+    std::vector<int> idx;
+    std::vector<double *> dst;
+    for (size_t c = a; c < outs.size(); ++c)
+      if (!done[c] && outs[c].nside == outs[a].nside) {
+        idx.push_back(outs[c].idx);
+        dst.push_back(outs[c].dst);
+        done[c] = true;
+      }
+    for (uint32_t s = 0; s < o.total_shell; ++s) {
+      const int st = interp_tab(h, outs[a].nside, o.nside_shell[s], &tab[s]);
+      if (st != HXG_OK) return st;
+    }
+    HXG_CK(launch_merge_all(h->stream, (int)outs[a].nside, (int)idx.size(), idx.data(),
+                            dst.data(), (int)o.total_shell, nside, b, tab));
+    h->launch_count += ((int64_t)idx.size() + kMaxMergeOuts - 1) / kMaxMergeOuts;
   }
   return HXG_OK;
 }
@@ -1424,15 +1530,16 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
   cudaSetDevice(h->device);
   int st = check_pass(h, o, d_dm, d_fd, d_is && d_qs && d_us);
   if (st != HXG_OK) return st;
-  const bool fp32 = h->precision == HXG_FP32C;
   uint32_t max_nside = 0;
   for (uint32_t s = 0; s < o->total_shell; ++s)
     max_nside = std::max(max_nside, o->nside_shell[s]);
   const size_t tbytes = npix_of(max_nside) * sizeof(double);
-  for (int k = 0; k < 5; ++k)
-    if ((st = ensure(h, h->tmp[k], tbytes)) != HXG_OK) return st;
-  double *tmp[5];
-  for (int k = 0; k < 5; ++k) tmp[k] = static_cast<double *>(h->tmp[k].p);
+  // the shell FD map is merged after each shell (the next one reads the
+  // accumulated FD); DM, I, Q, U of every shell are kept and merged at the end
+  if ((st = ensure(h, h->tmp[1], tbytes)) != HXG_OK) return st;
+  double *const tmp_fd = static_cast<double *>(h->tmp[1].p);
+  double *base[HXG_MAX_SHELLS];
+  if ((st = shell_blocks(h, *o, 4, base)) != HXG_OK) return st;
   // Grid_obs maps start at zero (Grid_obs::build_grid, grid_obs.cc:21-43)
   if (o->do_dm) HXG_CK(cudaMemsetAsync(d_dm, 0, npix_of(o->nside_dm) * 8, h->stream));
   if (o->do_fd) HXG_CK(cudaMemsetAsync(d_fd, 0, npix_of(o->nside_fd) * 8, h->stream));
@@ -1446,10 +1553,27 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
   if ((st = upload_ext(h, h->models, o->sync_freq, &ext_dev)) != HXG_OK) return st;
   const bool ck = h->checkpoint;
   for (uint32_t s = 0; s < o->total_shell; ++s) {
+    const size_t np = npix_of(o->nside_shell[s]);
+    double *const tmp[5] = {base[s], tmp_fd, base[s] + np, base[s] + 2 * np, base[s] + 3 * np};
     st = run_shell(h, *o, s, ext_dev, d_fd, tmp, 0, 1, ck);
     if (st != HXG_OK) return st;
-    if ((st = merge_shell(h, *o, s, tmp, d_dm, d_fd, d_is, d_qs, d_us)) != HXG_OK) return st;
+    if (o->do_fd) {
+      const double *src = tmp_fd;
+      InterpTab tab;
+      if ((st = interp_tab(h, o->nside_fd, o->nside_shell[s], &tab)) != HXG_OK) return st;
+      HXG_CK(launch_accumulate(h->stream, (int)o->nside_fd, (int)o->nside_shell[s], 1, &d_fd,
+                               &src, &tab));
+      ++h->launch_count;
+    }
   }
+  std::vector<PassOut> outs;
+  if (o->do_dm) outs.push_back({o->nside_dm, 0, d_dm});
+  if (o->do_sync) {
+    outs.push_back({o->nside_sync, 1, d_is});
+    outs.push_back({o->nside_sync, 2, d_qs});
+    outs.push_back({o->nside_sync, 3, d_us});
+  }
+  if ((st = merge_pass(h, *o, base, outs)) != HXG_OK) return st;
   if (ck) {
     h->ck_valid = true;
     h->ck_obs = *o;
@@ -1577,17 +1701,13 @@ int write_fused(hxg_handle *h, const hxg_obs_t *o, double *const *outs) {
   for (uint32_t s = 0; s < o0.total_shell; ++s) max_nside = std::max(max_nside, o0.nside_shell[s]);
   const size_t tbytes = npix_of(max_nside) * sizeof(double);
   int st;
-  for (int k = 0; k < 5; ++k)
-    if ((st = ensure(h, h->tmp[k], tbytes)) != HXG_OK) return st;
-  for (int k = 0; k < 3 * (NF - 1); ++k)
-    if ((st = ensure(h, h->tmp_multi[k], tbytes)) != HXG_OK) return st;
-  double *tmp_dm = static_cast<double *>(h->tmp[0].p);
-  double *tmp_fd = static_cast<double *>(h->tmp[1].p);
-  double *tmp_iqu[NF][3];
-  for (int j = 0; j < 3; ++j) tmp_iqu[0][j] = static_cast<double *>(h->tmp[2 + j].p);
-  for (int f = 1; f < NF; ++f)
-    for (int j = 0; j < 3; ++j)
-      tmp_iqu[f][j] = static_cast<double *>(h->tmp_multi[3 * (f - 1) + j].p);
+  // the shell FD map is merged after each shell (the next one reads the
+  // accumulated FD); the shared DM and each pass's I, Q, U of every shell
+  // (map 0 and maps 1 + 3 f + j of the shell's block) are merged at the end
+  if ((st = ensure(h, h->tmp[1], tbytes)) != HXG_OK) return st;
+  double *const tmp_fd = static_cast<double *>(h->tmp[1].p);
+  double *base[HXG_MAX_SHELLS];
+  if ((st = shell_blocks(h, o0, 1 + 3 * NF, base)) != HXG_OK) return st;
   // the pass outputs start at zero (Grid_obs::build_grid, grid_obs.cc:21-43);
   // the inner-shell FD is read from the first pass that accumulates FD
   bool any_fd = false;
@@ -1604,35 +1724,41 @@ int write_fused(hxg_handle *h, const hxg_obs_t *o, double *const *outs) {
   const ExtModels *ext_dev = nullptr;
   if ((st = upload_ext(h, h->models, o0.sync_freq, &ext_dev)) != HXG_OK) return st;
   for (uint32_t s = 0; s < o0.total_shell; ++s) {
+    const size_t np = npix_of(o0.nside_shell[s]);
+    double *tmp_iqu[NF][3];
+    for (int f = 0; f < NF; ++f)
+      for (int j = 0; j < 3; ++j) tmp_iqu[f][j] = base[s] + (size_t)(1 + 3 * f + j) * np;
     st = fused_shell<NF>(h, o, s, 0, 1, any_fd ? outs[5 * fd_pass + 1] : nullptr,
-                         any_fd ? (int)o[fd_pass].nside_fd : 0, ext_dev, tmp_dm, tmp_fd,
+                         any_fd ? (int)o[fd_pass].nside_fd : 0, ext_dev, base[s], tmp_fd,
                          tmp_iqu);
     if (st != HXG_OK) return st;
-    // each pass merges the shared DM / FD maps it asks for and its own
-    // I/Q/U: one merge launch per output Nside for all passes' maps
-    std::vector<std::pair<uint32_t, std::pair<double *, const double *>>> pairs;
-    for (int f = 0; f < NF; ++f) {
-      double *const *m = outs + 5 * f;
-      if (o[f].do_dm) pairs.push_back({o[f].nside_dm, {m[0], tmp_dm}});
-      if (o[f].do_fd) pairs.push_back({o[f].nside_fd, {m[1], tmp_fd}});
-      for (int j = 0; j < 3; ++j) pairs.push_back({o[f].nside_sync, {m[2 + j], tmp_iqu[f][j]}});
-    }
-    std::vector<bool> done(pairs.size(), false);
-    for (size_t a = 0; a < pairs.size(); ++a) {
-      if (done[a]) continue;
+    // every pass that asks for FD merges the shell FD map: one launch per
+    // FD output Nside
+    std::vector<bool> done(NF, false);
+    for (int a = 0; a < NF; ++a) {
+      if (!o[a].do_fd || done[a]) continue;
       std::vector<double *> d;
       std::vector<const double *> sr;
-      for (size_t b = a; b < pairs.size(); ++b)
-        if (!done[b] && pairs[b].first == pairs[a].first) {
-          d.push_back(pairs[b].second.first);
-          sr.push_back(pairs[b].second.second);
-          done[b] = true;
+      for (int c = a; c < NF; ++c)
+        if (o[c].do_fd && !done[c] && o[c].nside_fd == o[a].nside_fd) {
+          d.push_back(outs[5 * c + 1]);
+          sr.push_back(tmp_fd);
+          done[c] = true;
         }
-      HXG_CK(launch_accumulate(h->stream, (int)pairs[a].first, (int)o0.nside_shell[s],
-                               (int)d.size(), d.data(), sr.data()));
+      InterpTab tab;
+      if ((st = interp_tab(h, o[a].nside_fd, o0.nside_shell[s], &tab)) != HXG_OK) return st;
+      HXG_CK(launch_accumulate(h->stream, (int)o[a].nside_fd, (int)o0.nside_shell[s],
+                               (int)d.size(), d.data(), sr.data(), &tab));
       ++h->launch_count;
     }
   }
+  std::vector<PassOut> pouts;
+  for (int f = 0; f < NF; ++f) {
+    double *const *m = outs + 5 * f;
+    if (o[f].do_dm) pouts.push_back({o[f].nside_dm, 0, m[0]});
+    for (int j = 0; j < 3; ++j) pouts.push_back({o[f].nside_sync, 1 + 3 * f + j, m[2 + j]});
+  }
+  if ((st = merge_pass(h, o0, base, pouts)) != HXG_OK) return st;
   h->ck_valid = false;
   return HXG_OK;
 }
@@ -1967,6 +2093,12 @@ int hxg_sync(hxg_handle *h) {
   cudaSetDevice(h->device);
   HXG_CK(cudaStreamSynchronize(h->stream));
   HXG_CK(cudaGetLastError());
+  return HXG_OK;
+}
+
+int hxg_set_interp_cache(hxg_handle *h, uint64_t bytes) {
+  if (!h) return HXG_ERR_INVALID;
+  h->interp_limit = (size_t)bytes;
   return HXG_OK;
 }
 

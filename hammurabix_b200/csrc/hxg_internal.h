@@ -27,9 +27,20 @@ struct RfgBregGrid {
   double x_min, x_max, y_min, y_max, z_min, z_max;
 };
 
+// The bilinear interpolation of an Nside-nside_src map at every pixel of an
+// Nside-nside_dst map (hpx_interp_weights), made once per Nside pair: pix[i]
+// = the 4 source pixels of output pixel i, w[2 i] and w[2 i + 1] = weights
+// 0-1 and 2-3.  Source maps of up to 2^32 pixels.
+struct InterpTab {
+  const uint4 *pix = nullptr;
+  const double2 *w = nullptr;
+};
+cudaError_t launch_interp_table(cudaStream_t s, int nside_dst, int nside_src, uint4 *pix,
+                                double2 *w);
+// dst_k += src_k (interpolated when the Nsides differ, from tab when given)
 cudaError_t launch_accumulate(cudaStream_t s, int nside_dst, int nside_src,
                               int nmaps, double *const *dst,
-                              const double *const *src);
+                              const double *const *src, const InterpTab *tab = nullptr);
 cudaError_t launch_pix2ang(cudaStream_t s, int nside, uint64_t n,
                            double *theta, double *phi);
 cudaError_t launch_interpolate(cudaStream_t s, int nside, const double *map,
@@ -80,6 +91,15 @@ cudaError_t launch_deinterleave3(cudaStream_t s, uint64_t n, const double *src, 
                                  double *y, double *z);
 cudaError_t launch_interleave3(cudaStream_t s, uint64_t n, const double *x, const double *y,
                                const double *z, double *dst);
+// Outputs per merge launch (launch_accumulate, launch_merge_all).
+constexpr int kMaxMergeOuts = 12;
+// Merges the shell maps of a whole pass into nout outputs at one Nside:
+// shell s holds its maps in one block at base[s] (map j at
+// base[s] + j npix(nside[s])); dst[k] = the shell-ordered sum of map idx[k].
+// tab[s]: shell s's interpolation table (null members: computed in place).
+cudaError_t launch_merge_all(cudaStream_t s, int nside_dst, int nout, const int *idx,
+                             double *const *dst, int nshells, const int *nside,
+                             const double *const *base, const InterpTab *tab);
 cudaError_t launch_unpack_grad(cudaStream_t s, uint64_t n, const double *rec,
                                double *gbx, double *gby, double *gbz,
                                double *gne, double bscale);

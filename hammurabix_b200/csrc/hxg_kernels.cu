@@ -17,14 +17,65 @@ namespace hxg {
 // dst_k += src_k for up to kMaxMergeMaps map pairs sharing one (nside_dst,
 // nside_src); when the Nsides differ, src is interpolated at each dst
 // pixel's pointing (the pointing and the 4 weights once for all maps).
-constexpr int kMaxMergeMaps = 12;
+constexpr int kMaxMergeMaps = kMaxMergeOuts;
 struct MergeMaps {
   int n;
   double *dst[kMaxMergeMaps];
   const double *src[kMaxMergeMaps];
 };
 
-__global__ void accumulate_kernel(int nside_dst, int nside_src, MergeMaps M) {
+// hpx_interp_apply (Hampix::interpolate's weighted sum, hamdis.h:683-695)
+// with the map values read through the read-only path: the shell maps are
+// not written while a merge runs.  The same operations in the same order.
+__device__ __forceinline__ double interp_apply_nc(const double *map, const unsigned pix[4],
+                                                  const double wght[4]) {
+  double wtot = 0.0, res = 0.0;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const double val = __ldg(map + pix[c]);
+    if (val > kUndefTest) {
+      res += val * wght[c];
+      wtot += wght[c];
+    }
+  }
+  return (wtot == 0.0) ? kUndef : res / wtot;
+}
+
+// The 4 source pixels and weights of output pixel i: from the table when
+// there is one, else from the output pixel's pointing.
+__device__ __forceinline__ void interp_at(const InterpTab &T, const Hpx &hd, const Hpx &hs,
+                                          uint64_t i, uint64_t pix[4], double w[4]) {
+  if (T.pix) {
+    const uint4 p = __ldg(T.pix + i);
+    const double2 a = __ldg(T.w + 2 * i), b = __ldg(T.w + 2 * i + 1);
+    pix[0] = p.x;
+    pix[1] = p.y;
+    pix[2] = p.z;
+    pix[3] = p.w;
+    w[0] = a.x;
+    w[1] = a.y;
+    w[2] = b.x;
+    w[3] = b.y;
+    return;
+  }
+  double th, ph;
+  hpx_pix2ang(hd, i, th, ph);
+  hpx_interp_weights(hs, th, ph, pix, w);
+}
+
+__global__ void interp_table_kernel(int nside_dst, int nside_src, uint4 *tp, double2 *tw) {
+  const Hpx hd = hpx_make((uint64_t)nside_dst), hs = hpx_make((uint64_t)nside_src);
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= hd.npix) return;
+  uint64_t pix[4];
+  double w[4];
+  interp_at(InterpTab{}, hd, hs, i, pix, w);
+  tp[i] = make_uint4((unsigned)pix[0], (unsigned)pix[1], (unsigned)pix[2], (unsigned)pix[3]);
+  tw[2 * i] = make_double2(w[0], w[1]);
+  tw[2 * i + 1] = make_double2(w[2], w[3]);
+}
+
+__global__ void accumulate_kernel(int nside_dst, int nside_src, MergeMaps M, InterpTab T) {
   const Hpx hd = hpx_make((uint64_t)nside_dst);
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= hd.npix) return;
@@ -33,13 +84,77 @@ __global__ void accumulate_kernel(int nside_dst, int nside_src, MergeMaps M) {
     return;
   }
   const Hpx hs = hpx_make((uint64_t)nside_src);
-  double th, ph;
-  hpx_pix2ang(hd, i, th, ph);
   uint64_t pix[4];
   double w[4];
-  hpx_interp_weights(hs, th, ph, pix, w);
+  interp_at(T, hd, hs, i, pix, w);
+  const unsigned p32[4] = {(unsigned)pix[0], (unsigned)pix[1], (unsigned)pix[2],
+                           (unsigned)pix[3]};
   for (int k = 0; k < M.n; ++k)
-    M.dst[k][i] = M.dst[k][i] + hpx_interp_apply(M.src[k], pix, w);
+    M.dst[k][i] = M.dst[k][i] + interp_apply_nc(M.src[k], p32, w);
+}
+
+// All shells' maps merged into the pass outputs at once (the DM and Stokes
+// maps, whose merges no later shell waits for).  Shell s holds its maps in
+// one block at base[s], map j at base[s] + j npix(nside[s]); output k sums
+// map idx[k] of every shell, in shell order, at its pixel: directly where the
+// Nsides agree, else by HEALPix interpolation (Hampix::accumulate,
+// hamdis.h:698-721).  These are the additions of one accumulate per shell into
+// zeroed outputs, in the same order, with each output written once instead
+// of read and written per shell.
+struct MergeAll {
+  int n;        // outputs
+  int nshells;
+  int idx[kMaxMergeMaps];
+  int nside[HXG_MAX_SHELLS];
+  const double *base[HXG_MAX_SHELLS];
+  double *dst[kMaxMergeMaps];
+  InterpTab tab[HXG_MAX_SHELLS];
+};
+
+// One thread per output pixel walks the shells in order and keeps the
+// running sums in the outputs themselves (a thread's output lines stay in
+// cache from one shell to the next, so DRAM sees each output written about
+// once).  A shell's source pixels and weights come from its Nside pair's
+// interpolation table, or are found in place -- the same values: one
+// function makes both.  kTab: every interpolated shell has its table.
+template <bool kTab>
+__global__ void __launch_bounds__(256, 4) merge_all_kernel(int nside_dst, MergeAll M) {
+  const Hpx hd = hpx_make((uint64_t)nside_dst);
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= hd.npix) return;
+  for (int s = 0; s < M.nshells; ++s) {
+    const uint64_t ns = (uint64_t)M.nside[s];
+    const uint64_t npix = 12ull * ns * ns;
+    if (M.nside[s] == nside_dst) {
+      for (int k = 0; k < M.n; ++k) {
+        const double v = __ldg(M.base[s] + (uint64_t)M.idx[k] * npix + i);
+        M.dst[k][i] = (s == 0 ? 0. : M.dst[k][i]) + v;
+      }
+      continue;
+    }
+    unsigned pix[4];
+    double w[4];
+    if (kTab) {
+      const uint4 q = __ldg(M.tab[s].pix + i);
+      const double2 a = __ldg(M.tab[s].w + 2 * i), b = __ldg(M.tab[s].w + 2 * i + 1);
+      pix[0] = q.x;
+      pix[1] = q.y;
+      pix[2] = q.z;
+      pix[3] = q.w;
+      w[0] = a.x;
+      w[1] = a.y;
+      w[2] = b.x;
+      w[3] = b.y;
+    } else {
+      uint64_t p[4];
+      interp_at(InterpTab{}, hd, hpx_make(ns), i, p, w);
+      for (int c = 0; c < 4; ++c) pix[c] = (unsigned)p[c];
+    }
+    for (int k = 0; k < M.n; ++k) {
+      const double v = interp_apply_nc(M.base[s] + (uint64_t)M.idx[k] * npix, pix, w);
+      M.dst[k][i] = (s == 0 ? 0. : M.dst[k][i]) + v;
+    }
+  }
 }
 
 __global__ void pix2ang_kernel(int nside, uint64_t n, double *theta,
@@ -228,9 +343,17 @@ static inline unsigned blocks_for(uint64_t n, unsigned tpb) {
   return (unsigned)((n + tpb - 1) / tpb);
 }
 
+cudaError_t launch_interp_table(cudaStream_t s, int nside_dst, int nside_src, uint4 *pix,
+                                double2 *w) {
+  const uint64_t n = 12ull * nside_dst * nside_dst;
+  if (12ull * nside_src * nside_src > 0xffffffffull) return cudaErrorInvalidValue;
+  interp_table_kernel<<<blocks_for(n, 256), 256, 0, s>>>(nside_dst, nside_src, pix, w);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_accumulate(cudaStream_t s, int nside_dst, int nside_src,
                               int nmaps, double *const *dst,
-                              const double *const *src) {
+                              const double *const *src, const InterpTab *tab) {
   const uint64_t n = 12ull * nside_dst * nside_dst;
   for (int k0 = 0; k0 < nmaps; k0 += kMaxMergeMaps) {
     MergeMaps M{};
@@ -239,7 +362,38 @@ cudaError_t launch_accumulate(cudaStream_t s, int nside_dst, int nside_src,
       M.dst[k] = dst[k0 + k];
       M.src[k] = src[k0 + k];
     }
-    accumulate_kernel<<<blocks_for(n, 256), 256, 0, s>>>(nside_dst, nside_src, M);
+    accumulate_kernel<<<blocks_for(n, 256), 256, 0, s>>>(nside_dst, nside_src, M,
+                                                         tab ? *tab : InterpTab{});
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_merge_all(cudaStream_t s, int nside_dst, int nout, const int *idx,
+                             double *const *dst, int nshells, const int *nside,
+                             const double *const *base, const InterpTab *tab) {
+  if (nshells < 1 || nshells > HXG_MAX_SHELLS) return cudaErrorInvalidValue;
+  const uint64_t n = 12ull * nside_dst * nside_dst;
+  for (int k0 = 0; k0 < nout; k0 += kMaxMergeMaps) {
+    MergeAll M{};
+    M.n = nout - k0 < kMaxMergeMaps ? nout - k0 : kMaxMergeMaps;
+    M.nshells = nshells;
+    bool all_tab = true;
+    for (int sh = 0; sh < nshells; ++sh) {
+      M.nside[sh] = nside[sh];
+      M.base[sh] = base[sh];
+      if (tab) M.tab[sh] = tab[sh];
+      if (nside[sh] != nside_dst && !M.tab[sh].pix) all_tab = false;
+    }
+    for (int k = 0; k < M.n; ++k) {
+      M.idx[k] = idx[k0 + k];
+      M.dst[k] = dst[k0 + k];
+    }
+    if (all_tab)
+      merge_all_kernel<true><<<blocks_for(n, 256), 256, 0, s>>>(nside_dst, M);
+    else
+      merge_all_kernel<false><<<blocks_for(n, 256), 256, 0, s>>>(nside_dst, M);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

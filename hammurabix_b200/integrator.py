@@ -253,6 +253,11 @@ class Integrator:
         obs requests).  Returns a Batch; Batch.run() launches its graph."""
         return Batch(self, list(entries), tune)
 
+    def set_interp_cache(self, nbytes):
+        """Bound on the device bytes of the merges' interpolation tables
+        (hxg_set_interp_cache; 0: weights found in place)."""
+        _lib.check(self._lib.hxg_set_interp_cache(self._h, int(nbytes)), self._h)
+
     # ---- timing ----------------------------------------------------------
     def set_timing(self, enable=True):
         _lib.check(self._lib.hxg_set_timing(self._h, int(bool(enable))), self._h)

@@ -455,6 +455,18 @@ int hxg_get_timing(hxg_handle *h, double *kernel_ms, int64_t *launches,
 /* Total number of kernels this handle has launched (all kinds).          */
 int hxg_get_launch_count(hxg_handle *h, int64_t *count);
 
+/* ---- interpolation tables of the shell merges -------------------------
+ * No counterpart in the reference (Hampix::accumulate, hamdis.h:698-721,
+ * finds the interpolation weights of every output pixel on every call).  A
+ * shell map merged into an output of another Nside is interpolated at each
+ * output pixel; the handle keeps the 4 source pixels and weights of every
+ * output pixel per pair of Nsides (48 bytes per output pixel: 604 MB for
+ * Nside 1024), made on first use and held until hxg_destroy.  bytes bounds
+ * their total (default 8 GiB); pairs beyond it, or all of them when bytes
+ * is 0, find the weights in place.  The maps are the same either way.
+ * Lowering the bound frees no table already made.                        */
+int hxg_set_interp_cache(hxg_handle *h, uint64_t bytes);
+
 /* ---- allocation-free integration ---------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate
  * device memory -- plugins whose host application owns every device

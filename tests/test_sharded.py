@@ -294,3 +294,69 @@ def test_emulated_shards_of_fused_passes(fields32, nshards):
                 got = fd if k == "fd" else sum(outs[r][f][j] for r in range(nshards))
                 e = rel_err(got.cpu().numpy(), ref[f][j].cpu().numpy())
                 assert e <= 1e-5, (f, k, e)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_pass_end_merge_matches_per_shell_merges_bit_for_bit(fields32, precision):
+    """hxg_write_grid_device and hxg_write_grid_multi keep every shell's DM
+    and Stokes maps and merge them once at the end of the pass; the public
+    per-shell calls (one shard) merge after each shell.  Both add the same
+    shell values in the same order into zeroed outputs, so the maps agree
+    exactly: pass by pass (the one-pass kernel in both) and for the
+    Pipeline's three passes (fused in both in the FP32C form), with the
+    interpolation tables and without them."""
+    from hammurabix_b200.integrator import Integrator
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    bx, by, bz, ne = (torch.tensor(np.asarray(a, dtype=np.float64).reshape(-1), device=dev)
+                      for a in fields32)
+    z = lambda n: torch.zeros(n, dtype=torch.float64, device=dev) if n else None
+    maps = lambda o: [z(n) for n in abi.obs_output_sizes(o)[:2]] + \
+        [z(abi.obs_output_sizes(o)[2]) for _ in range(3)]
+    # shells below and at the output Nside 32
+    passes = W.frequency_passes(W.make_obs([8, 16, 32], 20.0, 0.05, freq_ghz=0.408),
+                                [0.408, 1.4, 30.0])
+    nmax = abi.npix(32)
+    with Integrator(precision) as integ:
+        integ.set_stream(stream.cuda_stream)
+        integ.set_models(W.grid_models())
+        integ.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(32), [bx, by, bz])
+        integ.upload_grid_device(abi.HXG_FIELD_TEREG, W.grid_desc(32), [ne])
+        whole = [maps(o) for o in passes]
+        integ.write_grid_multi_device(list(zip(passes, whole)))
+        per = [dict(zip(sharded.MAPS, maps(o))) for o in passes]
+        sharded.write_passes_sharded(integ, passes, per, sharded.make_shell_maps(nmax, z), 0, 1,
+                                     lambda t: None)
+        single, single_per = [], []
+        for o in passes:
+            m = maps(o)
+            integ.write_grid_device(o, *m)
+            single.append(m)
+            p = dict(zip(sharded.MAPS, maps(o)))
+            sharded.write_grid_sharded(integ, o, p, {k: z(nmax) for k in sharded.MAPS}, 0, 1,
+                                       lambda t: None)
+            single_per.append(p)
+        integ.sync()
+    # no interpolation tables: the merges find the weights in place
+    with Integrator(precision) as integ:
+        integ.set_stream(stream.cuda_stream)
+        integ.set_interp_cache(0)
+        integ.set_models(W.grid_models())
+        integ.upload_grid_device(abi.HXG_FIELD_BRND, W.grid_desc(32), [bx, by, bz])
+        integ.upload_grid_device(abi.HXG_FIELD_TEREG, W.grid_desc(32), [ne])
+        notab = [maps(o) for o in passes]
+        integ.write_grid_multi_device(list(zip(passes, notab)))
+        integ.sync()
+    for f, o in enumerate(passes):
+        req = sharded.requested(o)
+        for j, k in enumerate(sharded.MAPS):
+            if not req[k]:
+                continue
+            a = per[f][k].cpu().numpy()
+            assert np.abs(a).max() > 0, (f, k)
+            assert np.array_equal(whole[f][j].cpu().numpy(), a), (f, k, "passes")
+            assert np.array_equal(notab[f][j].cpu().numpy(), a), (f, k, "no tables")
+            assert np.array_equal(single[f][j].cpu().numpy(),
+                                  single_per[f][k].cpu().numpy()), (f, k, "one pass")
