@@ -630,11 +630,12 @@ def main():
     # ---- end to end through the host-buffer C ABI -----------------------------
     def e2e_leg(prec, nsteps_timed):
         """Step throughput through the host-buffer C ABI in form `prec`:
-        every step uploads its grids from pinned host memory and reads its
-        maps back inside the timed region."""
-        pinned = [torch.empty(t.numel(), dtype=torch.float64, pin_memory=True) for t in f64]
+        every step uploads its grids (the workload's FP32 grids, through
+        hxg_upload_grid_f32) from pinned host memory and reads its maps back
+        inside the timed region."""
+        pinned = [torch.empty(t.numel(), dtype=torch.float32, pin_memory=True) for t in f64]
         for p, t in zip(pinned, f64):
-            p.copy_(t)
+            p.copy_(t)   # exact: the values are FP32 numbers
         hosts = [p.numpy() for p in pinned]
         keys = ("dm", "fd", "is", "qs", "us")
 

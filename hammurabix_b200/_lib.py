@@ -25,6 +25,7 @@ SIGNATURES = {
     "hxg_set_models": (C.c_int, [_h, C.POINTER(abi.Models)]),
     "hxg_upload_grid": (C.c_int, [_h, C.c_int, C.POINTER(abi.GridDesc), _dp, _dp, _dp]),
     "hxg_upload_grid_device": (C.c_int, [_h, C.c_int, C.POINTER(abi.GridDesc), _vp, _vp, _vp]),
+    "hxg_upload_grid_f32": (C.c_int, [_h, C.c_int, C.POINTER(abi.GridDesc), _vp, _vp, _vp]),
     "hxg_set_mask": (C.c_int, [_h, C.c_uint32, _dp]),
     "hxg_write_grid": (C.c_int, [_h, C.POINTER(abi.Obs), _dp, _dp, _dp, _dp, _dp]),
     "hxg_write_grid_device": (C.c_int, [_h, C.POINTER(abi.Obs), _vp, _vp, _vp, _vp, _vp]),

@@ -72,8 +72,8 @@ struct hxg_handle {
   uint32_t mask_nside = 0;
   std::vector<double> mask_host;
   std::map<uint32_t, unsigned char *> mask_dev;
-  DevBuf tmp[5];
-  DevBuf tmp_multi[6];  // I/Q/U shell maps of the 2nd and 3rd fused pass
+  DevBuf tmp_fd;        // the shell FD map, merged after each shell
+  DevBuf stage32;       // staged chunk of an FP32 host grid
   DevBuf shell_all;     // every shell's DM and Stokes maps of a pass
   // interpolation tables by (output Nside << 32 | shell Nside)
   std::map<uint64_t, DevBuf> interp;
@@ -943,10 +943,8 @@ int hxg_destroy(hxg_handle *h) {
   for (auto &s : h->slots)
     for (auto &p : s.d)
       if (p) cudaFree(p);
-  for (auto &b : h->tmp)
-    if (b.p) cudaFree(b.p);
-  for (auto &b : h->tmp_multi)
-    if (b.p) cudaFree(b.p);
+  if (h->tmp_fd.p) cudaFree(h->tmp_fd.p);
+  if (h->stage32.p) cudaFree(h->stage32.p);
   if (h->shell_all.p) cudaFree(h->shell_all.p);
   for (auto &kv : h->interp) cudaFree(kv.second.p);
   for (auto &b : h->out)
@@ -998,6 +996,39 @@ int hxg_upload_grid(hxg_handle *h, int field, const hxg_grid_desc_t *g,
   cudaSetDevice(h->device);
   const int st = upload_common(h, field, g, c0, c1, c2, cudaMemcpyHostToDevice);
   if (st != HXG_OK) return st;
+  HXG_CK(cudaStreamSynchronize(h->stream));
+  return HXG_OK;
+}
+
+int hxg_upload_grid_f32(hxg_handle *h, int field, const hxg_grid_desc_t *g,
+                        const float *c0, const float *c1, const float *c2) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  const bool vec = field == HXG_FIELD_BREG || field == HXG_FIELD_BRND;
+  const float *src[3] = {c0, c1, c2};
+  for (int k = 0; k < (vec ? 3 : 1); ++k)
+    if (!src[k]) return fail(h, HXG_ERR_INVALID, "grid component %d is NULL", k);
+  size_t n;
+  int ncomp;
+  int st = slot_prepare(h, field, g, &n, &ncomp);
+  if (st != HXG_OK) return st;
+  // chunks of 2^26 values (256 MiB) staged on the device and widened into
+  // the slot, in stream order (the widening of a chunk takes about 1/40 of
+  // its copy)
+  const size_t chunk = (size_t)1 << 26;
+  if ((st = ensure(h, h->stage32, std::min(chunk, n) * sizeof(float))) != HXG_OK) return st;
+  float *stage = static_cast<float *>(h->stage32.p);
+  Slot &S = h->slots[field];
+  for (int k = 0; k < ncomp; ++k)
+    for (size_t off = 0; off < n; off += chunk) {
+      const size_t m = std::min(chunk, n - off);
+      HXG_CK(cudaMemcpyAsync(stage, src[k] + off, m * sizeof(float), cudaMemcpyHostToDevice,
+                             h->stream));
+      HXG_CK(launch_widen(h->stream, m, stage, S.d[k] + off));
+      ++h->launch_count;
+    }
+  S.present = true;
+  h->groups_dirty = true;
   HXG_CK(cudaStreamSynchronize(h->stream));
   return HXG_OK;
 }
@@ -1536,8 +1567,8 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
   const size_t tbytes = npix_of(max_nside) * sizeof(double);
   // the shell FD map is merged after each shell (the next one reads the
   // accumulated FD); DM, I, Q, U of every shell are kept and merged at the end
-  if ((st = ensure(h, h->tmp[1], tbytes)) != HXG_OK) return st;
-  double *const tmp_fd = static_cast<double *>(h->tmp[1].p);
+  if ((st = ensure(h, h->tmp_fd, tbytes)) != HXG_OK) return st;
+  double *const tmp_fd = static_cast<double *>(h->tmp_fd.p);
   double *base[HXG_MAX_SHELLS];
   if ((st = shell_blocks(h, *o, 4, base)) != HXG_OK) return st;
   // Grid_obs maps start at zero (Grid_obs::build_grid, grid_obs.cc:21-43)
@@ -1704,8 +1735,8 @@ int write_fused(hxg_handle *h, const hxg_obs_t *o, double *const *outs) {
   // the shell FD map is merged after each shell (the next one reads the
   // accumulated FD); the shared DM and each pass's I, Q, U of every shell
   // (map 0 and maps 1 + 3 f + j of the shell's block) are merged at the end
-  if ((st = ensure(h, h->tmp[1], tbytes)) != HXG_OK) return st;
-  double *const tmp_fd = static_cast<double *>(h->tmp[1].p);
+  if ((st = ensure(h, h->tmp_fd, tbytes)) != HXG_OK) return st;
+  double *const tmp_fd = static_cast<double *>(h->tmp_fd.p);
   double *base[HXG_MAX_SHELLS];
   if ((st = shell_blocks(h, o0, 1 + 3 * NF, base)) != HXG_OK) return st;
   // the pass outputs start at zero (Grid_obs::build_grid, grid_obs.cc:21-43);

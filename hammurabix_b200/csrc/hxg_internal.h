@@ -89,6 +89,7 @@ cudaError_t launch_batch_zero(cudaStream_t s, const ZeroJob *jobs,
                               unsigned long long nblocks);
 cudaError_t launch_deinterleave3(cudaStream_t s, uint64_t n, const double *src, double *x,
                                  double *y, double *z);
+cudaError_t launch_widen(cudaStream_t s, uint64_t n, const float *src, double *dst);
 cudaError_t launch_interleave3(cudaStream_t s, uint64_t n, const double *x, const double *y,
                                const double *z, double *dst);
 // Outputs per merge launch (launch_accumulate, launch_merge_all).

@@ -609,6 +609,20 @@ cudaError_t launch_interleave3(cudaStream_t s, uint64_t n, const double *x, cons
   return cudaGetLastError();
 }
 
+// FP32 values widened to FP64 (exact): an FP32 host grid's staged chunk
+// into its FP64 slot.
+__global__ void widen_kernel(uint64_t n, const float *src, double *dst) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  dst[i] = (double)src[i];
+}
+
+cudaError_t launch_widen(cudaStream_t s, uint64_t n, const float *src, double *dst) {
+  if (n == 0) return cudaSuccess;
+  widen_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, src, dst);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_batch_merge(cudaStream_t s, const MergeJob *jobs,
                                const unsigned long long *block0, int njobs,
                                unsigned long long nblocks) {

@@ -228,6 +228,12 @@ int hxg_set_models(hxg_handle *h, const hxg_models_t *m);
  * (HXG_ERR_INVALID otherwise).                                            */
 int hxg_upload_grid(hxg_handle *h, int field, const hxg_grid_desc_t *g,
                     const double *c0, const double *c1, const double *c2);
+/* Same, from host FP32 arrays (no counterpart in the reference, whose grids
+ * are FP64): the values are widened to FP64 on the device (exactly), so the
+ * slot and every map equal those of hxg_upload_grid with the same values as
+ * FP64, for half the host-to-device bytes.  Synchronous.                  */
+int hxg_upload_grid_f32(hxg_handle *h, int field, const hxg_grid_desc_t *g,
+                        const float *c0, const float *c1, const float *c2);
 /* Load a grid straight from the reference's binary grid file
  * (Grid_*::import_grid, source/grid/grid_breg.cc:48-66 and its tereg /
  * brnd / ternd / cre twins): raw native-endian FP64, the B slots with

@@ -69,3 +69,42 @@ def test_bad_files_are_rejected(tmp_path):
             with pytest.raises(_lib.HxgError) as e:
                 f.upload_grid_file(abi.HXG_FIELD_BRND, desc, str(path))
             assert e.value.status == abi.HXG_ERR_INVALID
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_fp32_host_grids_match_their_fp64_values(precision, fields32):
+    """hxg_upload_grid_f32 widens FP32 host grids on the device: the slots
+    and the maps equal those of hxg_upload_grid given the same values as
+    FP64 (bit for bit), in both forms."""
+    n = 32
+    desc = W.grid_desc(n)
+    b32 = [np.asarray(a, dtype=np.float32).reshape(-1) for a in fields32[:3]]
+    t32 = [np.asarray(fields32[3], dtype=np.float32).reshape(-1)]
+    o = W.make_obs([8, 16, 32], 20.0, 0.05, freq_ghz=1.4)
+    with I.Integrator(precision) as a, I.Integrator(precision) as f:
+        for ig, conv in ((a, lambda v: [x.astype(np.float64) for x in v]), (f, lambda v: v)):
+            ig.set_models(W.grid_models())
+            ig.upload_grid(abi.HXG_FIELD_BRND, desc, conv(b32))
+            ig.upload_grid(abi.HXG_FIELD_TEREG, desc, conv(t32))
+        for field in (abi.HXG_FIELD_BRND, abi.HXG_FIELD_TEREG):
+            for x, y in zip(a.download_grid(field, desc), f.download_grid(field, desc)):
+                np.testing.assert_array_equal(x, y)
+        ma, mf = a.write_grid(o), f.write_grid(o)
+        for k in ("dm", "fd", "is", "qs", "us"):
+            assert np.abs(ma[k]).max() > 0, k
+            np.testing.assert_array_equal(ma[k], mf[k])
+
+
+def test_fp32_host_grid_in_several_chunks():
+    # 420^3 = 74.1 M values: one full 2^26-value chunk and a partial one
+    n = 420
+    desc = W.grid_desc(n)
+    rng = np.random.Generator(np.random.PCG64(9))
+    t32 = rng.random(n ** 3, dtype=np.float32)
+    m = W.grid_models()
+    m.brnd = abi.HXG_BRND_NONE
+    with I.Integrator("fp32c") as f:
+        f.set_models(m)
+        f.upload_grid(abi.HXG_FIELD_TEREG, desc, [t32])
+        (got,) = f.download_grid(abi.HXG_FIELD_TEREG, desc)
+    np.testing.assert_array_equal(got.reshape(-1), t32.astype(np.float64))
