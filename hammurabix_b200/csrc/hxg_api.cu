@@ -74,6 +74,11 @@ struct hxg_handle {
   std::map<uint32_t, unsigned char *> mask_dev;
   DevBuf tmp_fd;        // the shell FD map, merged after each shell
   DevBuf stage32;       // staged chunk of an FP32 host grid
+  // FP32 host uploads: copies and widening on a stream of the greatest
+  // priority, so that the widening is not queued behind the blocks of an
+  // integration running on another stream
+  cudaStream_t up_stream = nullptr;
+  cudaEvent_t up_event = nullptr;
   DevBuf shell_all;     // every shell's DM and Stokes maps of a pass
   // interpolation tables by (output Nside << 32 | shell Nside)
   std::map<uint64_t, DevBuf> interp;
@@ -945,6 +950,8 @@ int hxg_destroy(hxg_handle *h) {
       if (p) cudaFree(p);
   if (h->tmp_fd.p) cudaFree(h->tmp_fd.p);
   if (h->stage32.p) cudaFree(h->stage32.p);
+  if (h->up_event) cudaEventDestroy(h->up_event);
+  if (h->up_stream) cudaStreamDestroy(h->up_stream);
   if (h->shell_all.p) cudaFree(h->shell_all.p);
   for (auto &kv : h->interp) cudaFree(kv.second.p);
   for (auto &b : h->out)
@@ -1013,23 +1020,35 @@ int hxg_upload_grid_f32(hxg_handle *h, int field, const hxg_grid_desc_t *g,
   int st = slot_prepare(h, field, g, &n, &ncomp);
   if (st != HXG_OK) return st;
   // chunks of 2^26 values (256 MiB) staged on the device and widened into
-  // the slot, in stream order (the widening of a chunk takes about 1/40 of
-  // its copy)
+  // the slot, in order on the upload stream (the widening of a chunk takes
+  // about 1/40 of its copy), after the work already queued on the handle's
+  // stream (which may still read the slot); the handle's stream then waits
+  // for the upload
   const size_t chunk = (size_t)1 << 26;
   if ((st = ensure(h, h->stage32, std::min(chunk, n) * sizeof(float))) != HXG_OK) return st;
+  if (!h->up_stream) {
+    int least = 0, greatest = 0;
+    HXG_CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    HXG_CK(cudaStreamCreateWithPriority(&h->up_stream, cudaStreamNonBlocking, greatest));
+    HXG_CK(cudaEventCreateWithFlags(&h->up_event, cudaEventDisableTiming));
+  }
+  HXG_CK(cudaEventRecord(h->up_event, h->stream));
+  HXG_CK(cudaStreamWaitEvent(h->up_stream, h->up_event, 0));
   float *stage = static_cast<float *>(h->stage32.p);
   Slot &S = h->slots[field];
   for (int k = 0; k < ncomp; ++k)
     for (size_t off = 0; off < n; off += chunk) {
       const size_t m = std::min(chunk, n - off);
       HXG_CK(cudaMemcpyAsync(stage, src[k] + off, m * sizeof(float), cudaMemcpyHostToDevice,
-                             h->stream));
-      HXG_CK(launch_widen(h->stream, m, stage, S.d[k] + off));
+                             h->up_stream));
+      HXG_CK(launch_widen(h->up_stream, m, stage, S.d[k] + off));
       ++h->launch_count;
     }
+  HXG_CK(cudaEventRecord(h->up_event, h->up_stream));
+  HXG_CK(cudaStreamWaitEvent(h->stream, h->up_event, 0));
   S.present = true;
   h->groups_dirty = true;
-  HXG_CK(cudaStreamSynchronize(h->stream));
+  HXG_CK(cudaEventSynchronize(h->up_event));
   return HXG_OK;
 }
 

@@ -231,7 +231,11 @@ int hxg_upload_grid(hxg_handle *h, int field, const hxg_grid_desc_t *g,
 /* Same, from host FP32 arrays (no counterpart in the reference, whose grids
  * are FP64): the values are widened to FP64 on the device (exactly), so the
  * slot and every map equal those of hxg_upload_grid with the same values as
- * FP64, for half the host-to-device bytes.  Synchronous.                  */
+ * FP64, for half the host-to-device bytes.  The copies and the widening
+ * run after the work already queued on the handle's stream, on a stream of
+ * the device's greatest priority (so an integration running on another
+ * handle's stream does not hold up the widening), and the handle's stream
+ * waits for them.  Synchronous: returns when the slot holds the values.   */
 int hxg_upload_grid_f32(hxg_handle *h, int field, const hxg_grid_desc_t *g,
                         const float *c0, const float *c1, const float *c2);
 /* Load a grid straight from the reference's binary grid file
