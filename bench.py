@@ -43,6 +43,11 @@ WORKLOADS = {
     # shells), about 15 ms per launch
     "profile": dict(nside_shells=[64, 128, 256, 512], r_max_kpc=30.0, res_kpc=0.01,
                     freqs_ghz=[0.408, 1.4, 30.0], grid_n=256, seeds=(3, 4)),
+    # config 3's shells and output Nside on 0.5-kpc rays and a 64^3 grid: the
+    # shell merges (the same launches and map sizes as config 3) take most
+    # of the step; the case the merge kernels are captured on
+    "merges": dict(nside_shells=[128, 256, 512, 1024], r_max_kpc=0.5, res_kpc=0.01,
+                   freqs_ghz=[0.408, 1.4, 30.0], grid_n=64, seeds=(3, 4)),
 }
 # The bounded sample both arms time like for like: the first frequency pass
 # (DM + FD + synchrotron) of the workload over its innermost shell only,
