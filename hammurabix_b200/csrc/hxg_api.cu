@@ -79,6 +79,7 @@ struct hxg_handle {
   // integration running on another stream
   cudaStream_t up_stream = nullptr;
   cudaEvent_t up_event = nullptr;
+  cudaEvent_t switch_event = nullptr;  // hxg_set_stream's hand-over
   DevBuf shell_all;     // every shell's DM and Stokes maps of a pass
   // interpolation tables by (output Nside << 32 | shell Nside)
   std::map<uint64_t, DevBuf> interp;
@@ -951,6 +952,7 @@ int hxg_destroy(hxg_handle *h) {
   if (h->tmp_fd.p) cudaFree(h->tmp_fd.p);
   if (h->stage32.p) cudaFree(h->stage32.p);
   if (h->up_event) cudaEventDestroy(h->up_event);
+  if (h->switch_event) cudaEventDestroy(h->switch_event);
   if (h->up_stream) cudaStreamDestroy(h->up_stream);
   if (h->shell_all.p) cudaFree(h->shell_all.p);
   for (auto &kv : h->interp) cudaFree(kv.second.p);
@@ -980,7 +982,18 @@ const char *hxg_last_error(const hxg_handle *h) {
 
 int hxg_set_stream(hxg_handle *h, void *stream) {
   if (!h) return HXG_ERR_INVALID;
-  h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+  cudaSetDevice(h->device);
+  cudaStream_t next = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+  if (next != h->stream) {
+    // the handle's device state (packed grids, interpolation tables, maps)
+    // may still be written by work queued on the previous stream: the new
+    // stream waits for it
+    if (!h->switch_event)
+      HXG_CK(cudaEventCreateWithFlags(&h->switch_event, cudaEventDisableTiming));
+    HXG_CK(cudaEventRecord(h->switch_event, h->stream));
+    HXG_CK(cudaStreamWaitEvent(next, h->switch_event, 0));
+  }
+  h->stream = next;
   return HXG_OK;
 }
 

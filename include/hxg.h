@@ -213,7 +213,9 @@ int hxg_create(int device, int precision, hxg_handle **out);
 int hxg_destroy(hxg_handle *h);
 const char *hxg_last_error(const hxg_handle *h);
 /* Launch on this CUDA stream (cudaStream_t passed as void*; NULL = the
- * handle's own stream).                                                   */
+ * handle's own stream).  Work the handle queued on its previous stream is
+ * ordered before its later work on the new one (an event wait); the
+ * previous stream must still exist when this is called.                   */
 int hxg_set_stream(hxg_handle *h, void *stream);
 
 /* ---- field models: replaces Pipeline::assemble_breg/tereg/cre model
