@@ -431,7 +431,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="config3", choices=sorted(WORKLOADS))
     ap.add_argument("--fp64-steps", type=int, default=1)
-    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--e2e-steps", type=int, default=16)
     ap.add_argument("--e2e64-steps", type=int, default=3)
     ap.add_argument("--sub-steps", type=int, default=5,
                     help="timed repetitions of the bounded sample in each GPU form")
