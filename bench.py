@@ -775,7 +775,11 @@ def main():
     ipv = profile_figure(prof_name, "warp_inst_per_valid_sample")
     # one traversal per shell serves all fused passes: its integrated samples
     # are those of one pass; launched one by one, every pass traverses
-    valid_trav = sum(W.valid_samples(passes[0])) * (1 if fused else len(passes))
+    # sharded (N > 1): this rank's launches covered its shard of the pixels;
+    # the library's per-launch sample counts give the shard's share
+    local_frac = ksamples / (samples_step * args.steps) if ksamples else 1.0
+    valid_trav = (sum(W.valid_samples(passes[0])) * (1 if fused else len(passes))
+                  * local_frac)
     valid_per_s = valid_trav * args.steps / (kms / 1e3) if kms > 0 else None
     clk_sum = clk.summary()
     mhz = clk_sum["sm_mhz"] if clk_sum else 1965.0
@@ -804,7 +808,8 @@ def main():
                 "kernel_samples_per_s": ksamples / (kms / 1e3) if kms > 0 else None}
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    # the CPU reference is timed at N = 1 only (the other ranks would wait)
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         host = [t.cpu().numpy() for t in f64]
         cb = cpu_baseline(wl, host)
         v = cb["samples"] / cb["seconds"][0]
