@@ -38,6 +38,10 @@ SIGNATURES = {
                                          C.POINTER(abi.GridDesc), _vp, _vp, _vp, _vp, _vp,
                                          _vp, _vp]),
     "hxg_set_checkpointing": (C.c_int, [_h, C.c_int]),
+    "hxg_adjoint_shard_begin": (C.c_int, [_h, C.POINTER(abi.Obs), C.c_uint32, C.c_uint32]),
+    "hxg_adjoint_shard_shell": (C.c_int, [_h, C.POINTER(abi.Obs), C.c_uint32, _vp, _vp, _vp,
+                                          _vp, _vp, _vp]),
+    "hxg_adjoint_shard_finish": (C.c_int, [_h, _vp, _vp, _vp, _vp, _vp]),
     "hxg_adjoint_device": (C.c_int, [_h, C.POINTER(abi.Obs), _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                      _vp, _vp, _vp]),
     "hxg_shell_ref": (C.c_int, [C.POINTER(abi.Obs), C.c_uint32, _dp, _dp,

@@ -78,7 +78,9 @@ shell_fp32c_adjoint_kernel(const AdjointLaunch A) {
   const int seg = lane >> P.log2_chunks;
   const int c = lane & (C - 1);
   const Hpx h = hpx_make((uint64_t)P.nside);
-  const unsigned long long nest = (unsigned long long)gw * (32 >> P.log2_chunks) + seg;
+  // shard `shard` of `nshards` of the shell (the forward's pixels)
+  const unsigned long long nest =
+      shard_nest(P, (unsigned long long)gw * (32 >> P.log2_chunks) + seg);
   const bool valid = nest < h.npix;
   uint64_t ring = 0;
   bool live = false;

@@ -100,6 +100,15 @@ struct hxg_handle {
   hxg_models_t ck_models{};
   std::vector<DevBuf> ck, ck_inner;
   std::vector<int> ck_chunks;
+  // checkpoints of per-shell forward calls (hxg_shell_integrate_device):
+  // which shells of pass ck_sobs, models ck_smodels and shard ck_shard of
+  // ck_nshards hold one, and the sharded adjoint's next shell (-1: none open)
+  std::vector<char> ck_shell;
+  hxg_obs_t ck_sobs{};
+  hxg_models_t ck_smodels{};
+  uint32_t ck_shard = 0, ck_nshards = 1;
+  int adj_next = -1;
+  bool adj_open = false;
   DevBuf grad_rec, grad_par, g_shell[5], g_fdmap;
   DevBuf ext;  // ExtModels block of the current launches
   DevBuf cre_tab;  // synchrotron tables + CRE energy tables
@@ -1638,6 +1647,9 @@ int hxg_write_grid_device(hxg_handle *h, const hxg_obs_t *o, double *d_dm,
   }
   if ((st = merge_pass(h, *o, base, outs)) != HXG_OK) return st;
   if (ck) {
+    // the per-shell checkpoints were overwritten
+    h->ck_shell.clear();
+    h->adj_open = false;
     h->ck_valid = true;
     h->ck_obs = *o;
     h->ck_models = h->models;
@@ -1918,7 +1930,22 @@ int hxg_shell_integrate_device(hxg_handle *h, const hxg_obs_t *o, uint32_t shell
   const ExtModels *ext_dev = nullptr;
   if ((st = upload_ext(h, h->models, o->sync_freq, &ext_dev)) != HXG_OK) return st;
   h->ck_valid = false;
-  return run_shell(h, *o, shell, ext_dev, d_fd, tmp, shard, nshards, false);
+  const bool ck = h->checkpoint;
+  if (ck && (shell == 0 || h->ck_shell.size() != o->total_shell ||
+             std::memcmp(&h->ck_sobs, o, sizeof(*o)) != 0 ||
+             std::memcmp(&h->ck_smodels, &h->models, sizeof(h->models)) != 0 ||
+             h->ck_shard != shard || h->ck_nshards != nshards)) {
+    h->ck_shell.assign(o->total_shell, 0);
+    h->ck_sobs = *o;
+    h->ck_smodels = h->models;
+    h->ck_shard = shard;
+    h->ck_nshards = nshards;
+  }
+  h->adj_next = -1;
+  h->adj_open = false;
+  st = run_shell(h, *o, shell, ext_dev, d_fd, tmp, shard, nshards, ck);
+  if (st == HXG_OK && ck) h->ck_shell[shell] = 1;
+  return st;
 }
 
 int hxg_shell_integrate_multi_device(hxg_handle *h, int npass, const hxg_obs_t *o,
@@ -1984,32 +2011,94 @@ int hxg_shell_merge_device(hxg_handle *h, const hxg_obs_t *o, uint32_t shell,
   return merge_shell(h, *o, shell, tmp, d_dm, d_fd, d_is, d_qs, d_us);
 }
 
-int hxg_set_checkpointing(hxg_handle *h, int enable) {
-  if (!h) return HXG_ERR_INVALID;
-  h->checkpoint = enable != 0;
-  h->ck_valid = false;
+}  // extern "C"
+
+namespace {
+
+// The adjoint of shell s for the pixels of shard `shard` of `nshards`
+// (integrator.cc:60-133 differentiated): the transposes of the shell merges
+// (integrator.cc:121-132) take dL/d(outputs) to dL/d(shell maps), with
+// g_fdmap the complete dL/d(accumulated FD map) of the shells outside s;
+// the kernel adds the shell's inner-FD gradients into gfd_target and the
+// grid-record and parameter gradients into the handle's accumulators.
+int adjoint_shell(hxg_handle *h, const hxg_obs_t &o, uint32_t s, uint32_t shard,
+                  uint32_t nshards, const ExtModels *ext_dev, const double *g_dm,
+                  const double *g_fdmap, const double *g_is, const double *g_qs,
+                  const double *g_us, double *gfd_target) {
+  const bool fp32 = h->precision == HXG_FP32C;
+  ShellLaunch F;
+  uint64_t step;
+  int st = build_launch(h, h->models, o, s, F, step);
+  if (st != HXG_OK) return st;
+  F.ext = ext_dev;
+  const int ns = (int)o.nside_shell[s];
+  const uint64_t npix = npix_of((uint32_t)ns);
+  double *gs[5];
+  for (int k = 0; k < 5; ++k) gs[k] = static_cast<double *>(h->g_shell[k].p);
+  for (int k = 0; k < 5; ++k)
+    HXG_CK(cudaMemsetAsync(gs[k], 0, npix * sizeof(double), h->stream));
+  // transposes of the shell merges (integrator.cc:121-132)
+  if (o.do_dm && g_dm)
+    HXG_CK(launch_accumulate_transpose(h->stream, (int)o.nside_dm, ns, g_dm, gs[0], 1.));
+  if (o.do_fd)
+    HXG_CK(launch_accumulate_transpose(h->stream, (int)o.nside_fd, ns, g_fdmap, gs[1], 1.));
+  if (o.do_sync) {
+    const double tc = F.tc_a * F.tc_a / F.tc_b;
+    const double *gsy[3] = {g_is, g_qs, g_us};
+    for (int k = 0; k < 3; ++k)
+      if (gsy[k])
+        HXG_CK(launch_accumulate_transpose(h->stream, (int)o.nside_sync, ns, gsy[k], gs[2 + k],
+                                           tc));
+  }
+  F.fdmap = o.do_fd ? g_fdmap : nullptr;  // non-null marks inner-FD use
+  F.nside_fdmap = o.do_fd ? (int)o.nside_fd : 0;
+  F.mask = nullptr;
+  if (o.do_mask) {
+    const unsigned char *dmk = nullptr;
+    if ((st = device_mask(h, o.nside_shell[s], &dmk)) != HXG_OK) return st;
+    F.mask = dmk;
+  }
+  const int C = h->ck_chunks[s];
+  F.chunks = C;
+  F.log2_chunks = hpx_ilog2((uint64_t)C);
+  F.shard = shard;
+  F.nshards = nshards;
+  F.shard_log2 = shard_block_log2(npix, nshards);
+  const uint64_t bsz = 1ull << F.shard_log2;
+  const uint64_t nblk = (npix + bsz - 1) / bsz;
+  const uint64_t local = nshards == 1 ? npix : (nblk + nshards - 1 - shard) / nshards * bsz;
+  if (fp32 && !fast_models(F))
+    return fail(h, HXG_ERR_UNSUPPORTED,
+                "the FP32C adjoint covers the grid workloads' models (spiral or no regular "
+                "B, exponential disk or no regular n_e, CRE_ana with a constant index, no "
+                "inner radius cut); run the FP64 form");
+  AdjointLaunch A{};
+  A.F = F;
+  A.ck = static_cast<const double *>(h->ck[s].p);
+  A.ck_inner = static_cast<const double *>(h->ck_inner[s].p);
+  for (int k = 0; k < 5; ++k) A.g[k] = gs[k];
+  const size_t ngrid = h->groups.empty() ? 0 : h->groups[0].n;
+  A.grad_rec = ngrid ? static_cast<double *>(h->grad_rec.p) : nullptr;
+  A.grad_par = static_cast<double *>(h->grad_par.p);
+  A.g_fdmap = o.do_fd ? gfd_target : nullptr;
+  A.want_j0 = (h->models.cre == HXG_CRE_ANA || h->models.cre == HXG_CRE_UNIF) ? 1 : 0;
+  if (local == 0) return HXG_OK;
+  const uint64_t warps = (local + (32 / C) - 1) / (32 / C);
+  const unsigned threads = fp32 ? HXG_ADJ32_THREADS : HXG_ADJ_THREADS;
+  const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
+  HXG_CK(fp32 ? launch_adjoint32(h->stream, A, blocks, threads)
+              : launch_adjoint(h->stream, A, blocks, threads));
+  ++h->launch_count;
   return HXG_OK;
 }
 
-// Reverse-mode pass over the shells of the last checkpointed forward call
-// (integrator.cc:23-228 differentiated): outer shells first, so that the
-// inner-shell Faraday-depth gradients of shell s reach shells < s.
-int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
-                       const double *g_fd, const double *g_is,
-                       const double *g_qs, const double *g_us,
-                       double *d_grad_params, double *d_grad_bx,
-                       double *d_grad_by, double *d_grad_bz,
-                       double *d_grad_ne) {
-  if (!h || !o) return HXG_ERR_INVALID;
-  cudaSetDevice(h->device);
-  const bool fp32 = h->precision == HXG_FP32C;
-  if (!h->ck_valid || std::memcmp(&h->ck_obs, o, sizeof(*o)) != 0 ||
-      std::memcmp(&h->ck_models, &h->models, sizeof(h->models)) != 0)
-    return fail(h, HXG_ERR_STATE,
-                "no checkpointed forward pass for these obs/models (enable "
-                "hxg_set_checkpointing and call hxg_write_grid_device first)");
+// Checks and zeroed accumulators of a reverse-mode pass: the grid-record
+// and parameter gradients and the per-shell gradient maps.
+int adjoint_prepare(hxg_handle *h, const hxg_obs_t &o) {
   if (h->groups.size() > 1)
     return fail(h, HXG_ERR_UNSUPPORTED, "the adjoint supports one grid geometry");
+  if (h->models.cre == HXG_CRE_GRID)
+    return fail(h, HXG_ERR_UNSUPPORTED, "the adjoint does not cover the CRE-grid emissivity");
   int st;
   const size_t ngrid = h->groups.empty() ? 0 : h->groups[0].n;
   if (ngrid) {
@@ -2018,81 +2107,20 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
   }
   if ((st = ensure(h, h->grad_par, kNumParams * sizeof(double))) != HXG_OK) return st;
   HXG_CK(cudaMemsetAsync(h->grad_par.p, 0, kNumParams * sizeof(double), h->stream));
-  double *gfdmap = nullptr;
-  if (o->do_fd) {
-    const size_t b = npix_of(o->nside_fd) * sizeof(double);
-    if ((st = ensure(h, h->g_fdmap, b)) != HXG_OK) return st;
-    gfdmap = static_cast<double *>(h->g_fdmap.p);
-    if (g_fd)
-      HXG_CK(cudaMemcpyAsync(gfdmap, g_fd, b, cudaMemcpyDeviceToDevice, h->stream));
-    else
-      HXG_CK(cudaMemsetAsync(gfdmap, 0, b, h->stream));
-  }
   uint32_t max_nside = 0;
-  for (uint32_t s = 0; s < o->total_shell; ++s) max_nside = std::max(max_nside, o->nside_shell[s]);
+  for (uint32_t s = 0; s < o.total_shell; ++s) max_nside = std::max(max_nside, o.nside_shell[s]);
   for (int k = 0; k < 5; ++k)
     if ((st = ensure(h, h->g_shell[k], npix_of(max_nside) * sizeof(double))) != HXG_OK)
       return st;
-  double *gs[5];
-  for (int k = 0; k < 5; ++k) gs[k] = static_cast<double *>(h->g_shell[k].p);
-  if (h->models.cre == HXG_CRE_GRID)
-    return fail(h, HXG_ERR_UNSUPPORTED, "the adjoint does not cover the CRE-grid emissivity");
-  const ExtModels *ext_dev = nullptr;
-  if ((st = upload_ext(h, h->models, o->sync_freq, &ext_dev)) != HXG_OK) return st;
-  for (int s = (int)o->total_shell - 1; s >= 0; --s) {
-    ShellLaunch F;
-    uint64_t step;
-    if ((st = build_launch(h, h->models, *o, (uint32_t)s, F, step)) != HXG_OK) return st;
-    F.ext = ext_dev;
-    const int ns = (int)o->nside_shell[s];
-    const uint64_t npix = npix_of((uint32_t)ns);
-    for (int k = 0; k < 5; ++k)
-      HXG_CK(cudaMemsetAsync(gs[k], 0, npix * sizeof(double), h->stream));
-    // transposes of the shell merges (integrator.cc:121-132)
-    if (o->do_dm && g_dm)
-      HXG_CK(launch_accumulate_transpose(h->stream, (int)o->nside_dm, ns, g_dm, gs[0], 1.));
-    if (o->do_fd)
-      HXG_CK(launch_accumulate_transpose(h->stream, (int)o->nside_fd, ns, gfdmap, gs[1], 1.));
-    if (o->do_sync) {
-      const double tc = F.tc_a * F.tc_a / F.tc_b;
-      const double *gsy[3] = {g_is, g_qs, g_us};
-      for (int k = 0; k < 3; ++k)
-        if (gsy[k])
-          HXG_CK(launch_accumulate_transpose(h->stream, (int)o->nside_sync, ns, gsy[k],
-                                             gs[2 + k], tc));
-    }
-    F.fdmap = o->do_fd ? gfdmap : nullptr;  // non-null marks inner-FD use
-    F.nside_fdmap = o->do_fd ? (int)o->nside_fd : 0;
-    F.mask = nullptr;
-    if (o->do_mask) {
-      const unsigned char *dmk = nullptr;
-      if ((st = device_mask(h, o->nside_shell[s], &dmk)) != HXG_OK) return st;
-      F.mask = dmk;
-    }
-    const int C = h->ck_chunks[s];
-    F.chunks = C;
-    F.log2_chunks = hpx_ilog2((uint64_t)C);
-    if (fp32 && !fast_models(F))
-      return fail(h, HXG_ERR_UNSUPPORTED,
-                  "the FP32C adjoint covers the grid workloads' models (spiral or no regular "
-                  "B, exponential disk or no regular n_e, CRE_ana with a constant index, no "
-                  "inner radius cut); run the FP64 form");
-    AdjointLaunch A{};
-    A.F = F;
-    A.ck = static_cast<const double *>(h->ck[s].p);
-    A.ck_inner = static_cast<const double *>(h->ck_inner[s].p);
-    for (int k = 0; k < 5; ++k) A.g[k] = gs[k];
-    A.grad_rec = ngrid ? static_cast<double *>(h->grad_rec.p) : nullptr;
-    A.grad_par = static_cast<double *>(h->grad_par.p);
-    A.g_fdmap = gfdmap;
-    A.want_j0 = (h->models.cre == HXG_CRE_ANA || h->models.cre == HXG_CRE_UNIF) ? 1 : 0;
-    const uint64_t warps = (npix + (32 / C) - 1) / (32 / C);
-    const unsigned threads = fp32 ? HXG_ADJ32_THREADS : HXG_ADJ_THREADS;
-    const unsigned blocks = (unsigned)((warps * 32 + threads - 1) / threads);
-    HXG_CK(fp32 ? launch_adjoint32(h->stream, A, blocks, threads)
-                : launch_adjoint(h->stream, A, blocks, threads));
-    ++h->launch_count;
-  }
+  return HXG_OK;
+}
+
+// dL/d(parameters) and dL/d(grid values) from the handle's accumulators
+// (the grid records unpacked into the slots' SoA layout and units).
+int adjoint_finish(hxg_handle *h, double *d_grad_params, double *d_grad_bx, double *d_grad_by,
+                   double *d_grad_bz, double *d_grad_ne) {
+  const bool fp32 = h->precision == HXG_FP32C;
+  const size_t ngrid = h->groups.empty() ? 0 : h->groups[0].n;
   // parameter gradients: j0 slot holds sum (dL/dJ) J, divide by j0
   double gp[kNumParams];
   HXG_CK(cudaMemcpyAsync(gp, h->grad_par.p, sizeof(gp), cudaMemcpyDeviceToHost, h->stream));
@@ -2121,6 +2149,114 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
   }
   HXG_CK(cudaStreamSynchronize(h->stream));
   return HXG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hxg_set_checkpointing(hxg_handle *h, int enable) {
+  if (!h) return HXG_ERR_INVALID;
+  h->checkpoint = enable != 0;
+  h->ck_valid = false;
+  h->ck_shell.clear();
+  h->adj_next = -1;
+  h->adj_open = false;
+  return HXG_OK;
+}
+
+int hxg_adjoint_shard_begin(hxg_handle *h, const hxg_obs_t *o, uint32_t shard,
+                            uint32_t nshards) {
+  if (!h || !o) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  bool all = h->ck_shell.size() == o->total_shell && o->total_shell > 0;
+  for (char c : h->ck_shell) all = all && c;
+  if (!all || std::memcmp(&h->ck_sobs, o, sizeof(*o)) != 0 ||
+      std::memcmp(&h->ck_smodels, &h->models, sizeof(h->models)) != 0 ||
+      h->ck_shard != shard || h->ck_nshards != nshards)
+    return fail(h, HXG_ERR_STATE,
+                "no checkpointed per-shell forward pass of shard %u of %u for these obs/models "
+                "(enable hxg_set_checkpointing and call hxg_shell_integrate_device for every "
+                "shell first)", shard, nshards);
+  const int st = adjoint_prepare(h, *o);
+  if (st != HXG_OK) return st;
+  h->adj_next = (int)o->total_shell - 1;
+  h->adj_open = true;
+  return HXG_OK;
+}
+
+int hxg_adjoint_shard_shell(hxg_handle *h, const hxg_obs_t *o, uint32_t shell,
+                            const double *g_dm, const double *g_fdmap, const double *g_is,
+                            const double *g_qs, const double *g_us, double *d_gfd_inc) {
+  if (!h || !o) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  if (!h->adj_open || std::memcmp(&h->ck_sobs, o, sizeof(*o)) != 0)
+    return fail(h, HXG_ERR_STATE, "no sharded adjoint open for these obs (hxg_adjoint_shard_begin)");
+  if (shell >= o->total_shell || (int)shell != h->adj_next)
+    return fail(h, HXG_ERR_INVALID, "shell %u out of order: the adjoint runs shell %d next "
+                "(outermost first)", shell, h->adj_next);
+  if (o->do_fd && (!g_fdmap || !d_gfd_inc))
+    return fail(h, HXG_ERR_INVALID, "an FD pass needs g_fdmap and the increment map");
+  if (o->do_fd)
+    HXG_CK(cudaMemsetAsync(d_gfd_inc, 0, npix_of(o->nside_fd) * sizeof(double), h->stream));
+  const ExtModels *ext_dev = nullptr;
+  int st = upload_ext(h, h->models, o->sync_freq, &ext_dev);
+  if (st != HXG_OK) return st;
+  st = adjoint_shell(h, *o, shell, h->ck_shard, h->ck_nshards, ext_dev, g_dm,
+                     o->do_fd ? g_fdmap : nullptr, g_is, g_qs, g_us,
+                     o->do_fd ? d_gfd_inc : nullptr);
+  if (st != HXG_OK) return st;
+  --h->adj_next;
+  return HXG_OK;
+}
+
+int hxg_adjoint_shard_finish(hxg_handle *h, double *d_grad_params, double *d_grad_bx,
+                             double *d_grad_by, double *d_grad_bz, double *d_grad_ne) {
+  if (!h) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  if (!h->adj_open || h->adj_next != -1)
+    return fail(h, HXG_ERR_STATE, "the sharded adjoint has shells left or was not begun");
+  h->adj_open = false;
+  h->ck_shell.clear();  // one reverse pass per forward pass
+  return adjoint_finish(h, d_grad_params, d_grad_bx, d_grad_by, d_grad_bz, d_grad_ne);
+}
+
+// Reverse-mode pass over the shells of the last checkpointed forward call
+// (integrator.cc:23-228 differentiated): outer shells first, so that the
+// inner-shell Faraday-depth gradients of shell s reach shells < s.
+int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *o, const double *g_dm,
+                       const double *g_fd, const double *g_is,
+                       const double *g_qs, const double *g_us,
+                       double *d_grad_params, double *d_grad_bx,
+                       double *d_grad_by, double *d_grad_bz,
+                       double *d_grad_ne) {
+  if (!h || !o) return HXG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  if (!h->ck_valid || std::memcmp(&h->ck_obs, o, sizeof(*o)) != 0 ||
+      std::memcmp(&h->ck_models, &h->models, sizeof(h->models)) != 0)
+    return fail(h, HXG_ERR_STATE,
+                "no checkpointed forward pass for these obs/models (enable "
+                "hxg_set_checkpointing and call hxg_write_grid_device first)");
+  int st = adjoint_prepare(h, *o);
+  if (st != HXG_OK) return st;
+  double *gfdmap = nullptr;
+  if (o->do_fd) {
+    const size_t b = npix_of(o->nside_fd) * sizeof(double);
+    if ((st = ensure(h, h->g_fdmap, b)) != HXG_OK) return st;
+    gfdmap = static_cast<double *>(h->g_fdmap.p);
+    if (g_fd)
+      HXG_CK(cudaMemcpyAsync(gfdmap, g_fd, b, cudaMemcpyDeviceToDevice, h->stream));
+    else
+      HXG_CK(cudaMemsetAsync(gfdmap, 0, b, h->stream));
+  }
+  const ExtModels *ext_dev = nullptr;
+  if ((st = upload_ext(h, h->models, o->sync_freq, &ext_dev)) != HXG_OK) return st;
+  for (int s = (int)o->total_shell - 1; s >= 0; --s) {
+    st = adjoint_shell(h, *o, (uint32_t)s, 0, 1, ext_dev, g_dm, gfdmap, g_is, g_qs, g_us,
+                       gfdmap);
+    if (st != HXG_OK) return st;
+  }
+  return adjoint_finish(h, d_grad_params, d_grad_bx, d_grad_by, d_grad_bz, d_grad_ne);
 }
 
 int hxg_write_grid(hxg_handle *h, const hxg_obs_t *o, double *dm, double *fd,

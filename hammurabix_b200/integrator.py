@@ -253,6 +253,29 @@ class Integrator:
             self._h, C.byref(obs), ptr(g_dm), ptr(g_fd), ptr(g_is), ptr(g_qs), ptr(g_us),
             ptr(grad_params), ptr(gb[0]), ptr(gb[1]), ptr(gb[2]), ptr(grad_ne)))
 
+    # ---- sharded adjoint (one rank's part; sharded.adjoint_sharded) ---------
+    def adjoint_shard_begin(self, obs, shard, nshards):
+        """hxg_adjoint_shard_begin: after write_grid_sharded's per-shell
+        forward of shard `shard` of `nshards` with checkpointing on."""
+        self._ordered(lambda: self._lib.hxg_adjoint_shard_begin(
+            self._h, C.byref(obs), int(shard), int(nshards)))
+
+    def adjoint_shard_shell(self, obs, shell, g_dm, g_fdmap, g_is, g_qs, g_us, gfd_inc):
+        """hxg_adjoint_shard_shell (outermost shell first): gfd_inc receives
+        this shard's inner-FD terms of the shell."""
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        self._ordered(lambda: self._lib.hxg_adjoint_shard_shell(
+            self._h, C.byref(obs), int(shell), ptr(g_dm), ptr(g_fdmap), ptr(g_is), ptr(g_qs),
+            ptr(g_us), ptr(gfd_inc)))
+
+    def adjoint_shard_finish(self, grad_params=None, grad_b=None, grad_ne=None):
+        """hxg_adjoint_shard_finish: this shard's gradients (their sum over
+        the shards is the full gradient)."""
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        gb = list(grad_b) if grad_b is not None else [None, None, None]
+        self._ordered(lambda: self._lib.hxg_adjoint_shard_finish(
+            self._h, ptr(grad_params), ptr(gb[0]), ptr(gb[1]), ptr(gb[2]), ptr(grad_ne)))
+
     # ---- batched forward ---------------------------------------------------
     def batch(self, entries, tune=False):
         """Plan a batch of independent passes sharing this handle's grids.

@@ -15,6 +15,11 @@ pass (a reduce, not an all-reduce: no rank but the first needs them), so
 after a pass rank 0 holds every output map and the other ranks the FD map
 and their own partial DM / I / Q / U.  Every rank issues the same
 collectives in the same order.
+
+The adjoint of such a pass (adjoint_sharded) runs each rank's pixels shell
+by shell from the outermost, with the mirror exchange: the ranks sum their
+terms of dL/d(accumulated FD map) after each shell, and all-reduce the grid
+and parameter gradients at the end.
 """
 from . import abi
 
@@ -65,6 +70,44 @@ def write_grid_sharded(integ, obs, outs, tmp, rank, world, reduce_sum, reduce_ro
         for k in ("dm", "is", "qs", "us"):
             if req[k]:
                 reduce_root(outs[k])
+
+
+def adjoint_sharded(integ, obs, g, grads, rank, world, reduce_sum, zeros):
+    """The reverse pass of a pass that write_grid_sharded ran on this rank
+    with checkpointing on (Integrator.set_checkpointing): the gradients of a
+    scalar loss of the maps, the multi-GPU form of hxg_adjoint_device.
+
+    Each rank runs the adjoint of its own pixels, shell by shell from the
+    outermost.  The one exchange mirrors the forward's: every pixel of an
+    inner shell read the accumulated FD map, so its gradient dL/d(FD map)
+    collects terms from every pixel of the outer shells; after each shell
+    the ranks sum their terms (reduce_sum) and add them to the map before
+    the next shell.  At the end each rank holds its pixels' share of the
+    grid and parameter gradients, summed over the ranks (reduce_sum: the
+    grid-gradient all-reduce).
+
+    g: dict of dL/d(outputs) keyed like MAPS (torch CUDA float64, None =
+    zero); grads: dict "params" (HXG_NUM_PARAMS doubles), "b" (3 tensors or
+    None), "ne" (tensor or None), filled with the full gradient on every
+    rank; zeros(n): a zeroed float64 buffer of n elements on the device."""
+    integ.adjoint_shard_begin(obs, rank, world)
+    gfd = inc = None
+    if obs.do_fd:
+        n = abi.npix(obs.nside_fd)
+        gfd = g["fd"].clone() if g.get("fd") is not None else zeros(n)
+        inc = zeros(n)
+    for s in reversed(range(obs.total_shell)):
+        integ.adjoint_shard_shell(obs, s, g.get("dm"), gfd, g.get("is"), g.get("qs"),
+                                  g.get("us"), inc)
+        if inc is not None:
+            if world > 1:
+                reduce_sum(inc)
+            gfd += inc
+    integ.adjoint_shard_finish(grads.get("params"), grads.get("b"), grads.get("ne"))
+    if world > 1:
+        for t in [grads.get("params"), grads.get("ne")] + list(grads.get("b") or []):
+            if t is not None:
+                reduce_sum(t)
 
 
 def make_shell_maps(n, zeros):

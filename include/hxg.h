@@ -412,6 +412,33 @@ int hxg_adjoint_device(hxg_handle *h, const hxg_obs_t *obs,
                        double *d_grad_bx, double *d_grad_by,
                        double *d_grad_bz, double *d_grad_ne);
 
+/* ---- sharded adjoint (the multi-GPU form of the above) -------------------
+ * No counterpart in the reference.  One rank's part of the reverse pass
+ * of a pass whose forward ran shell by shell on shard `shard` of `nshards`
+ * (hxg_shell_integrate_device with checkpointing on, every shell, the
+ * same obs and models).  The ranks exchange what the unsharded adjoint
+ * keeps in one map: dL/d(accumulated FD map), which every pixel of the
+ * inner shells reads.
+ *  - hxg_adjoint_shard_begin: checks the checkpoints and zeroes the
+ *    gradient accumulators.
+ *  - hxg_adjoint_shard_shell, shells from the outermost to the innermost:
+ *    g_dm / g_is / g_qs / g_us as in hxg_adjoint_device; g_fdmap = the
+ *    complete dL/d(FD output) including the inner-FD terms of all outer
+ *    shells (the same on every rank; start from dL/d(FD output));
+ *    d_gfd_inc (npix(nside_fd) doubles) receives this shard's inner-FD
+ *    terms of this shell.  Before the next shell the caller sums d_gfd_inc
+ *    over the ranks and adds it to g_fdmap.  FD passes need both maps.
+ *  - hxg_adjoint_shard_finish: this shard's gradients in the outputs of
+ *    hxg_adjoint_device; their sum over the ranks is the full gradient.
+ * Launches on the handle's stream; finish synchronizes it.                */
+int hxg_adjoint_shard_begin(hxg_handle *h, const hxg_obs_t *obs, uint32_t shard,
+                            uint32_t nshards);
+int hxg_adjoint_shard_shell(hxg_handle *h, const hxg_obs_t *obs, uint32_t shell,
+                            const double *g_dm, const double *g_fdmap, const double *g_is,
+                            const double *g_qs, const double *g_us, double *d_gfd_inc);
+int hxg_adjoint_shard_finish(hxg_handle *h, double *d_grad_params, double *d_grad_bx,
+                             double *d_grad_by, double *d_grad_bz, double *d_grad_ne);
+
 /* ---- batched forward ---------------------------------------------------
  * Many independent passes -- parameter sets x frequencies, each one
  * Integrator::write_grid call (source/integrator/integrator.cc:23-134)

@@ -74,6 +74,30 @@ class FakeIntegrator:
             g = torch.Generator().manual_seed(len(o) * 7919 + len(t))
             o += torch.rand(len(o), len(t), generator=g, dtype=torch.float64) @ t
 
+    # the sharded adjoint's contract: a shell's terms come from this shard's
+    # pixels only and depend on the complete dL/d(FD map) of the outer
+    # shells; the gradient accumulators are sums over the pixels
+    def adjoint_shard_begin(self, obs, shard, nshards):
+        self._shard = (shard, nshards)
+        self._acc = torch.zeros(8 + 4 * 5, dtype=torch.float64)
+
+    def adjoint_shard_shell(self, obs, s, g_dm, g_fdmap, g_is, g_qs, g_us, inc):
+        n = abi.npix(obs.nside_shell[s])
+        own = torch.from_numpy(_owned(n, *self._shard)).double()
+        w = own * (1.0 + s + 0.01 * torch.arange(n, dtype=torch.float64))
+        level = 1.0 + 1e-3 * float(g_fdmap.sum()) + 1e-4 * float(g_is.sum())
+        g = torch.Generator().manual_seed(len(inc) * 104729 + n)
+        inc.zero_()
+        inc += (torch.rand(len(inc), n, generator=g, dtype=torch.float64) @ w) * level
+        g2 = torch.Generator().manual_seed(n)
+        self._acc += (torch.rand(len(self._acc), n, generator=g2, dtype=torch.float64) @ w) * level
+
+    def adjoint_shard_finish(self, params, b, ne):
+        params.copy_(self._acc[:8])
+        for k, t in enumerate(b):
+            t.copy_(self._acc[8 + 5 * k:13 + 5 * k])
+        ne.copy_(self._acc[23:28])
+
 
 def _obs():
     return W.make_obs([4, 8, 8], 20.0, 0.1, freq_ghz=1.4)
@@ -103,6 +127,19 @@ def _run_passes(world, rank, reduce_sum, reduce_root=None):
     return [{k: v.numpy().copy() for k, v in o.items()} for o in outs]
 
 
+def _run_adjoint(world, rank, reduce_sum):
+    o = _obs()
+    z = lambda n: torch.zeros(n, dtype=torch.float64)
+    ndm, nfd, nsy = abi.obs_output_sizes(o)
+    gen = torch.Generator().manual_seed(3)
+    g = {k: torch.rand(c, generator=gen, dtype=torch.float64)
+         for k, c in zip(sharded.MAPS, (ndm, nfd, nsy, nsy, nsy))}
+    grads = {"params": z(8), "b": [z(5) for _ in range(3)], "ne": z(5)}
+    sharded.adjoint_sharded(FakeIntegrator(), o, g, grads, rank, world, reduce_sum, z)
+    return np.concatenate([grads["params"].numpy()] + [t.numpy() for t in grads["b"]] +
+                          [grads["ne"].numpy()])
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -117,18 +154,21 @@ def _rank(rank, ws, port, q):
     w, r, _ = replicas.init("gloo", 60)
     red = lambda t: dist.all_reduce(t)
     root = lambda t: dist.reduce(t, dst=0)
-    q.put((r, (_run(w, r, red, root), _run_passes(w, r, red, root))))
+    q.put((r, (_run(w, r, red, root), _run_passes(w, r, red, root), _run_adjoint(w, r, red))))
     replicas.finish(w)
 
 
 def test_two_gloo_ranks_reproduce_the_single_process_pass():
-    """One pass (per-shell exchange) and three fused passes of the
-    Pipeline's order, on two ranks, against one process: rank 0 ends with
+    """One pass (per-shell exchange), three fused passes of the Pipeline's
+    order and the sharded adjoint of the one pass (per-shell exchange of
+    the FD-map gradient, all-reduced gradients), on two ranks, against one
+    process: every rank ends with the single process's gradients; rank 0 ends with
     every map of the single process (the DM and Stokes maps reduced onto
     it), every rank with the complete FD map, and rank 1's DM and Stokes
     maps stay its own shard's partial maps (no all-reduce at the end)."""
     single = _run(1, 0, None)
     single_multi = _run_passes(1, 0, None)
+    single_adj = _run_adjoint(1, 0, None)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
@@ -140,7 +180,10 @@ def test_two_gloo_ranks_reproduce_the_single_process_pass():
         p.join(timeout=60)
         assert p.exitcode == 0
     for r in (0, 1):
-        one, multi = got[r]
+        one, multi, adj = got[r]
+        # the sharded adjoint: every rank ends with the full gradient
+        assert np.abs(single_adj).max() > 0
+        assert rel_err(adj, single_adj) <= 1e-12, r
         for k in sharded.MAPS:
             assert np.abs(single[k]).max() > 0, k
             if r == 0 or k == "fd":
@@ -360,3 +403,109 @@ def test_pass_end_merge_matches_per_shell_merges_bit_for_bit(fields32, precision
             assert np.array_equal(notab[f][j].cpu().numpy(), a), (f, k, "no tables")
             assert np.array_equal(single[f][j].cpu().numpy(),
                                   single_per[f][k].cpu().numpy()), (f, k, "one pass")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32c", 1e-5)])
+@pytest.mark.parametrize("nshards", [2, 3])
+def test_emulated_sharded_adjoint_matches_the_unsplit_adjoint(precision, tol, nshards):
+    """The sharded adjoint (hxg_adjoint_shard_*) with the shards emulated one
+    after another on one GPU, one handle per shard as one per GPU: the
+    per-shell forward with its FD exchange and checkpoints, then the
+    reverse pass with the per-shell sum of the shards' FD-map gradient
+    terms; the shards' gradients summed (the all-reduce) against
+    hxg_adjoint_device on one handle.  Spiral B + exponential n_e disk +
+    CRE_ana with B and n_e random grids, 0.408 GHz with DM and FD (inner-
+    shell Faraday rotation), random dL/d(maps)."""
+    from hammurabix_b200.integrator import Integrator
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    n = 16
+    obs = W.make_obs([4, 8, 16], 24.0, 0.1, freq_ghz=0.408)
+    m = W.spiral_models()
+    m.brnd = abi.HXG_BRND_GRID
+    m.ternd = abi.HXG_TERND_GRID
+    desc = W.grid_desc(n)
+    rng = np.random.Generator(np.random.PCG64(21))
+    b = [torch.tensor(rng.standard_normal(n ** 3) * 0.5e-6, device=dev) for _ in range(3)]
+    ne = torch.tensor(0.01 * rng.standard_normal(n ** 3), device=dev)
+    z = lambda k: torch.zeros(k, dtype=torch.float64, device=dev)
+    ndm, nfd, nsy = abi.obs_output_sizes(obs)
+    g = {k: torch.tensor(rng.standard_normal(c), device=dev)
+         for k, c in zip(sharded.MAPS, (ndm, nfd, nsy, nsy, nsy))}
+
+    def handle():
+        ig = Integrator(precision)
+        ig.set_stream(stream.cuda_stream)
+        ig.set_models(m)
+        ig.upload_grid_device(abi.HXG_FIELD_BRND, desc, b)
+        ig.upload_grid_device(abi.HXG_FIELD_TERND, desc, [ne])
+        ig.set_checkpointing(True)
+        return ig
+
+    def grads():
+        return {"params": z(abi.HXG_NUM_PARAMS), "b": [z(n ** 3) for _ in range(3)],
+                "ne": z(n ** 3)}
+
+    ref = handle()
+    ref.write_grid_device(obs, z(ndm), z(nfd), z(nsy), z(nsy), z(nsy))
+    rg = grads()
+    ref.adjoint_device(obs, *[g[k] for k in sharded.MAPS], grad_params=rg["params"],
+                       grad_b=rg["b"], grad_ne=rg["ne"])
+    igs = [handle() for _ in range(nshards)]
+    # forward: per shell, every shard's shell maps, their sum (the all-reduce
+    # of the FD map) merged into the FD output every shard reads
+    fd = z(nfd)
+    nmax = abi.npix(max(obs.nside_shell[s] for s in range(obs.total_shell)))
+    for s in range(obs.total_shell):
+        ns = abi.npix(obs.nside_shell[s])
+        parts = []
+        for r, ig in enumerate(igs):
+            t = [z(nmax)[:ns] for _ in sharded.MAPS]
+            ig.shell_integrate_device(obs, s, r, nshards, fd, t)
+            parts.append(t)
+        tsum = [sum(p[j] for p in parts) for j in range(5)]
+        igs[0].shell_merge_device(obs, s, tsum, [z(ndm), fd, z(nsy), z(nsy), z(nsy)])
+    # reverse pass
+    for r, ig in enumerate(igs):
+        ig.adjoint_shard_begin(obs, r, nshards)
+    gfd = g["fd"].clone()
+    for s in reversed(range(obs.total_shell)):
+        incs = [z(nfd) for _ in igs]
+        for ig, inc in zip(igs, incs):
+            ig.adjoint_shard_shell(obs, s, g["dm"], gfd, g["is"], g["qs"], g["us"], inc)
+        gfd += sum(incs)
+    tot = grads()
+    for ig in igs:
+        part = grads()
+        ig.adjoint_shard_finish(part["params"], part["b"], part["ne"])
+        tot["params"] += part["params"]
+        tot["ne"] += part["ne"]
+        for k in range(3):
+            tot["b"][k] += part["b"][k]
+    torch.cuda.synchronize()
+    pairs = [("params", tot["params"], rg["params"]), ("ne", tot["ne"], rg["ne"])] + \
+        [(f"b{k}", tot["b"][k], rg["b"][k]) for k in range(3)]
+    for name, a, r in pairs:
+        a, r = a.cpu().numpy(), r.cpu().numpy()
+        assert np.abs(r).max() > 0, name
+        assert rel_err(a, r) <= tol, (name, rel_err(a, r))
+    # parameters one by one (their scales differ by orders of magnitude; the
+    # FP32C shards split rays over other lane counts than the unsplit pass)
+    a, r = tot["params"].cpu().numpy(), rg["params"].cpu().numpy()
+    ptol = tol if precision == "fp64" else 1e-4
+    for k in range(abi.HXG_NUM_PARAMS):
+        assert abs(a[k] - r[k]) <= ptol * abs(r[k]) + 1e-300, (k, a[k], r[k])
+    # one reverse pass per forward pass; a finish without a begin is refused
+    from hammurabix_b200._lib import HxgError
+    with pytest.raises(HxgError) as e:
+        igs[0].adjoint_shard_begin(obs, 0, nshards)
+    assert e.value.status == abi.HXG_ERR_STATE
+    with pytest.raises(HxgError):
+        igs[0].adjoint_shard_finish(z(abi.HXG_NUM_PARAMS))
+    # the whole-pass forward leaves no per-shell checkpoints
+    with pytest.raises(HxgError):
+        ref.adjoint_shard_begin(obs, 0, 1)
+    for ig in [ref] + igs:
+        ig.close()
