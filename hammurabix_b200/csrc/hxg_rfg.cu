@@ -44,10 +44,13 @@ __host__ __device__ inline void philox4x32_10(uint32_t ctr[4], uint32_t k0, uint
 }
 
 // Four standard normal deviates for cell idx: two Philox blocks give four
-// 53-bit uniforms in (0, 1), two Box-Muller pairs turn them into normals.
+// 53-bit uniforms in (0, 1), two Box-Muller pairs turn them into normals;
+// nb = 1: the first pair only (from the first block), the same two values.
+template <int nb = 2>
 __device__ inline void gauss4(uint64_t seed, uint64_t idx, double g[4]) {
   double u[4];
-  for (int b = 0; b < 2; ++b) {
+#pragma unroll
+  for (int b = 0; b < nb; ++b) {
     uint32_t c[4] = {(uint32_t)idx, (uint32_t)(idx >> 32), (uint32_t)b, 0x52464721u};
     philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
     for (int q = 0; q < 2; ++q) {
@@ -55,7 +58,8 @@ __device__ inline void gauss4(uint64_t seed, uint64_t idx, double g[4]) {
       u[2 * b + q] = ((double)(w & ((1ull << 53) - 1)) + 0.5) * 0x1p-53;
     }
   }
-  for (int q = 0; q < 2; ++q) {
+#pragma unroll
+  for (int q = 0; q < nb; ++q) {
     const double r = sqrt(-2. * log(u[2 * q]));
     double s, c;
     sincospi(2. * u[2 * q + 1], &s, &c);
@@ -85,8 +89,16 @@ __device__ inline double spec_es(double k, const hxg_brnd_es_t &p) {
   const double band1 = double(k < p.k1);
   const double band2 = double(k > p.k1) * double(k < p.k0);
   const double band3 = double(k > p.k0);
-  const double P = band1 * pow(p.k0 / p.k1, p.a1) * pow(k / p.k1, 6.) +
-                   band2 / pow(k / p.k0, p.a1) + band3 / pow(k / p.k0, p.a0);
+  // the band that holds k, the others adding exact zeros: the value of
+  // band1 * A * B + band2 / C + band3 / D with one or none of its terms
+  // evaluated
+  double P = 0.;
+  if (band1 != 0.)
+    P = band1 * pow(p.k0 / p.k1, p.a1) * pow(k / p.k1, 6.);
+  else if (band2 != 0.)
+    P = band2 / pow(k / p.k0, p.a1);
+  else if (band3 != 0.)
+    P = band3 / pow(k / p.k0, p.a0);
   return P * p0 * unit;
 }
 
@@ -127,7 +139,10 @@ __global__ void rfg_fill_kernel(RfgGrid G, int kind, hxg_ternd_dft_t pt, hxg_brn
   const double kx = kcomp(i, G.nx, G.lx), ky = kcomp(j, G.ny, G.ly), kz = kcomp(l, G.nz, G.lz);
   const double ks = sqrt(kx * kx + ky * ky + kz * kz);
   double g[4];
-  gauss4(seed, idx, g);
+  if (kind == 0)
+    gauss4<1>(seed, idx, g);
+  else
+    gauss4<2>(seed, idx, g);
   if (kind == 0) {
     const double sigma = sqrt(spec_dft(ks, pt) * G.dk3);
     c0[idx] = make_double2(sigma * g[0], sigma * g[1]);
