@@ -102,12 +102,14 @@ __device__ inline double spec_es(double k, const hxg_brnd_es_t &p) {
   return P * p0 * unit;
 }
 
-// spatial_profile (ternd_dft.cc:26-33, brnd_es.cc:46-52)
-__device__ inline double profile(double x, double y, double z, const double obs[3], double r0,
-                                 double z0) {
+// The square root of spatial_profile (ternd_dft.cc:26-33, brnd_es.cc:46-52),
+// exp(-r_cyl / r0) exp(-zz / z0), that both rescales take: one exponential
+// of half the summed exponent (equal to rounding).
+__device__ inline double sqrt_profile(double x, double y, double z, const double obs[3],
+                                      double r0, double z0) {
   const double r_cyl = sqrt(x * x + y * y) - fabs(obs[0]);
   const double zz = fabs(z) - fabs(obs[2]);
-  return exp(-r_cyl / r0) * exp(-zz / z0);
+  return exp(-0.5 * (r_cyl / r0 + zz / z0));
 }
 
 struct RfgGrid {
@@ -185,7 +187,7 @@ __global__ void ternd_rescale_kernel(RfgGrid G, hxg_ternd_dft_t p, double obs0, 
   const double x = i * G.lx / (G.nx - 1) + G.xmin;
   const double y = j * G.ly / (G.ny - 1) + G.ymin;
   const double z = l * G.lz / (G.nz - 1) + G.zmin;
-  const double ratio = sqrt(profile(x, y, z, obs, p.r0, p.z0)) * p.rms * var_invsq;
+  const double ratio = sqrt_profile(x, y, z, obs, p.r0, p.z0) * p.rms * var_invsq;
   te[idx] = c[idx].x * ratio;
 }
 
@@ -239,7 +241,7 @@ __global__ void brnd_rescale_kernel(RfgGrid G, hxg_brnd_es_t p, DevModels M,
   const double x = i * G.lx / (G.nx - 1) + G.xmin;
   const double y = j * G.ly / (G.ny - 1) + G.ymin;
   const double z = l * G.lz / (G.nz - 1) + G.zmin;
-  const double ratio = sqrt(profile(x, y, z, M.obs, p.r0, p.z0)) * p.rms * var_invsq;
+  const double ratio = sqrt_profile(x, y, z, M.obs, p.r0, p.z0) * p.rms * var_invsq;
   const double2 a0 = c0[idx], a1 = c1[idx];
   const double b[3] = {a0.x * ratio, a0.y * ratio, a1.y * ratio};
   const double p3[3] = {x, y, z};
