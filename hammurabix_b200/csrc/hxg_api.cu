@@ -2610,6 +2610,7 @@ int batch_tables(hxg_batch *b, int lanes, int grain) {
     for (auto &t : t0) t.assign(1, 0ull);
     std::vector<MergeJob> mj;
     std::vector<unsigned long long> m0(1, 0ull);
+    int tab_st = HXG_OK;
     const auto job = [&](int nmaps, double *const *d, const double *const *src, uint32_t nd,
                          int ns) {
       MergeJob J{};
@@ -2620,6 +2621,8 @@ int batch_tables(hxg_batch *b, int lanes, int grain) {
       J.nmaps = nmaps;
       J.nside_dst = (int)nd;
       J.nside_src = ns;
+      const int ts = interp_tab(h, nd, (uint32_t)ns, &J.tab);
+      if (ts != HXG_OK) tab_st = ts;
       mj.push_back(J);
       m0.push_back(m0.back() + (npix_of(nd) + 255) / 256);
     };
@@ -2718,6 +2721,7 @@ int batch_tables(hxg_batch *b, int lanes, int grain) {
     b->nplans[c0] = (int)P1.size();
     b->nplans[c0 + 1] = (int)P2.size();
     b->nplans[c0 + 2] = (int)P3.size();
+    if (tab_st != HXG_OK) return tab_st;
     b->nmerge[s] = (int)mj.size();
     b->merge_blocks[s] = m0.back();
     if ((st = upload_vec(h, b->plans[c0], P1)) != HXG_OK) return st;

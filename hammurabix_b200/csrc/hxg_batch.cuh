@@ -9,6 +9,7 @@
 
 #include "hxg_fp32c.cuh"
 #include "hxg_integrate.cuh"
+#include "hxg_internal.h"
 
 namespace hxg {
 
@@ -139,6 +140,7 @@ struct MergeJob {
   double *dst[3];
   const double *src[3];
   int nmaps, nside_dst, nside_src, _pad;
+  InterpTab tab;  // the Nside pair's interpolation table (null: in place)
 };
 
 // Zeroing of every output map of the batch (Grid_obs maps start at zero,

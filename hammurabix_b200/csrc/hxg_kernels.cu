@@ -323,13 +323,13 @@ __global__ void batch_merge_kernel(const MergeJob *jobs,
     return;
   }
   const Hpx hs = hpx_make((uint64_t)J.nside_src);
-  double th, ph;
-  hpx_pix2ang(hd, i, th, ph);
   uint64_t pix[4];
   double w[4];
-  hpx_interp_weights(hs, th, ph, pix, w);
+  interp_at(J.tab, hd, hs, i, pix, w);
+  const unsigned p32[4] = {(unsigned)pix[0], (unsigned)pix[1], (unsigned)pix[2],
+                           (unsigned)pix[3]};
   for (int k = 0; k < J.nmaps; ++k)
-    J.dst[k][i] = J.dst[k][i] + hpx_interp_apply(J.src[k], pix, w);
+    J.dst[k][i] = J.dst[k][i] + interp_apply_nc(J.src[k], p32, w);
 }
 
 __global__ void batch_zero_kernel(const ZeroJob *jobs,
