@@ -660,61 +660,80 @@ def main():
             ig_.upload_grid(abi.HXG_FIELD_BRND, desc, hosts[:3])
             ig_.upload_grid(abi.HXG_FIELD_TEREG, desc, hosts[3:])
 
+        # sharded (N > 1): every rank takes the same collective steps in the
+        # same order -- one handle, one stream, steps one after another,
+        # device maps read back by torch copies
+        e2e_streams = [stream]
+        iges, e2e_outs, pinned_outs = [], [], []
         if shard:
-            # every rank takes the same collective steps in the same order:
-            # one handle, one stream, steps one after another
-            e2e_streams = [stream]
-        else:
-            # two handles on two streams and a read-back stream: step k+1's
-            # grids cross PCIe (the upload returns when its copies are done)
-            # while step k computes, and step k's maps come back (the other
-            # direction) while step k+1 computes; every step still uploads
-            # its own grids and reads back its own maps inside the timed
-            # region
-            e2e_streams = [stream, torch.cuda.Stream(dev)]
-        rb_stream = torch.cuda.Stream(dev)
-        iges = [e2e_integ(s) for s in e2e_streams]
-        e2e_outs = [outputs() for _ in iges]
-        pinned_outs = [[{k: torch.empty(npx, dtype=torch.float64, pin_memory=True).numpy()
-                         for k in keys} for _ in passes] for _ in iges]
+            iges = [e2e_integ(s) for s in e2e_streams]
+            e2e_outs = [outputs() for _ in iges]
+            pinned_outs = [[{k: torch.empty(npx, dtype=torch.float64, pin_memory=True).numpy()
+                             for k in keys} for _ in passes] for _ in iges]
 
         def e2e_run(nsteps):
-            npipe = len(iges)
-            comp = [None] * npipe   # per handle: its last step's compute is done
-            home = [None] * npipe   # per handle: its last step's maps are home
-            upload(iges[0])
+            ig_, s_ = iges[0], e2e_streams[0]
+            upload(ig_)
             for k in range(nsteps):
-                a, b = k % npipe, (k + 1) % npipe
-                sa = e2e_streams[a]
-                if npipe == 1:
-                    with torch.cuda.stream(sa):
-                        step(iges[a], e2e_outs[a])
-                        read_back(e2e_outs[a], pinned_outs[a])
-                    sa.synchronize()
-                    if k + 1 < nsteps:
-                        upload(iges[a])
-                    continue
-                with torch.cuda.stream(sa):
-                    if home[a] is not None:
-                        sa.wait_event(home[a])   # step k-2's maps have left the outputs
-                    step(iges[a], e2e_outs[a])
-                    comp[a] = torch.cuda.Event()
-                    comp[a].record(sa)
-                rb_stream.wait_event(comp[a])
-                with torch.cuda.stream(rb_stream):
-                    read_back(e2e_outs[a], pinned_outs[a])
-                    home[a] = torch.cuda.Event()
-                    home[a].record(rb_stream)
+                with torch.cuda.stream(s_):
+                    step(ig_, e2e_outs[0])
+                    read_back(e2e_outs[0], pinned_outs[0])
+                s_.synchronize()
                 if k + 1 < nsteps:
-                    if comp[b] is not None:
-                        comp[b].synchronize()    # step k-1 no longer reads b's grids
-                    upload(iges[b])
+                    upload(ig_)
             torch.cuda.synchronize(dev)
 
-        e2e_run(2)
+        # one process per GPU, N = 1 (the replicas mode too): the host-buffer
+        # C ABI, as a host application calls it -- hxg_upload_grid_f32 from
+        # pinned host grids and hxg_write_grid_multi_host into pinned host
+        # maps, each call returning when its copies are done -- with two
+        # handles driven by two host threads, so that one handle's upload
+        # and read-back cross PCIe while the other one computes
+        host_outs = ([[{k: torch.empty(npx, dtype=torch.float64, pin_memory=True).numpy()
+                        for k in keys} for _ in passes] for _ in range(2)]
+                     if not shard else [])
+
+        def e2e_run_host(nsteps):
+            import threading
+            errs = []
+            first_up = threading.Event()
+
+            def worker(t):
+                try:
+                    ig_ = host_iges[t]
+                    if t == 1:
+                        first_up.wait()     # stagger: handle 1 uploads while 0 computes
+                    for k in range(t, nsteps, 2):
+                        upload(ig_)
+                        if k == 0:
+                            first_up.set()
+                        ig_.write_grid_multi(passes, out=host_outs[t])
+                except BaseException as e:  # noqa: BLE001 -- re-raised below
+                    errs.append(e)
+                    first_up.set()
+            ths = [threading.Thread(target=worker, args=(t,)) for t in range(2)]
+            for th in ths:
+                th.start()
+            for th in ths:
+                th.join()
+            if errs:
+                raise errs[0]
+
+        use_host = not shard
+        if use_host:
+            host_iges = []
+            for _ in range(2):
+                ig_ = Integrator(prec, device=local)
+                ig_.set_models(models)
+                host_iges.append(ig_)
+            iges = host_iges
+            run = e2e_run_host
+        else:
+            run = e2e_run
+        run(2)
         barrier()
         te0 = time.perf_counter()
-        e2e_run(nsteps_timed)
+        run(nsteps_timed)
         barrier()
         te = max_over_ranks((time.perf_counter() - te0) / nsteps_timed)
         h2d = sum(h.nbytes for h in hosts)
@@ -723,12 +742,15 @@ def main():
         res = {"value": (1 if shard else ws) * samples_step / te, "unit": UNIT,
                "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": te * 1e3,
-               "overlap": ("two handles on two streams and a read-back stream: step k+1's "
-                           "upload and step k-1's read-back overlap step k") if len(iges) > 1
+               "api": ("hxg_upload_grid_f32 + hxg_write_grid_multi_host (host buffers)"
+                       if use_host else
+                       "hxg_upload_grid_f32 + sharded write_grid (device maps, torch D2H)"),
+               "overlap": ("two handles driven by two host threads: one handle's upload and "
+                           "read-back overlap the other's compute") if use_host
                else "none"}
         for ig_ in iges:
             ig_.close()
-        del pinned, hosts, pinned_outs
+        del pinned, hosts, pinned_outs, host_outs
         log(f"[rank {rank}] e2e {prec}: {te * 1e3:.1f} ms/step")
         return res
 

@@ -174,18 +174,24 @@ class Integrator:
     def sync(self):
         _lib.check(self._lib.hxg_sync(self._h), self._h)
 
-    def write_grid_multi(self, passes):
+    def write_grid_multi(self, passes, out=None):
         """hxg_write_grid_multi_host: passes is a list of Obs; returns one
         dict dm/fd/is/qs/us of float64 numpy maps per pass (None where the
-        pass writes no such map)."""
+        pass writes no such map).  ``out`` may supply them (one dict per
+        pass of C-contiguous float64 arrays of the right sizes, e.g. pinned
+        memory), as in write_grid."""
         keys = ("dm", "fd", "is", "qs", "us")
         n = len(passes)
         obs = (abi.Obs * n)(*passes)
+        given = out
         out, ptrs = [], (C.c_void_p * (5 * n))()
         for k, o in enumerate(passes):
             ndm, nfd, nsy = abi.obs_output_sizes(o)
-            maps = {key: (np.zeros(c) if c else None)
-                    for key, c in zip(keys, (ndm, nfd, nsy, nsy, nsy))}
+            sizes = (ndm, nfd, nsy, nsy, nsy)
+            if given is None:
+                maps = {key: (np.zeros(c) if c else None) for key, c in zip(keys, sizes)}
+            else:
+                maps = {key: (given[k][key][:c] if c else None) for key, c in zip(keys, sizes)}
             for j, key in enumerate(keys):
                 if maps[key] is not None:
                     ptrs[5 * k + j] = maps[key].ctypes.data
