@@ -11,6 +11,10 @@ process -- each shard's shell maps summed the way the all-reduce sums them --
 against the unsplit hxg_write_grid_device: to rounding in FP64 (a shard has
 fewer pixels, so it may split each ray over more lanes, which regroups the
 sums) and to the FP32C tolerance.
+
+The sharded adjoint (sharded.adjoint_sharded, hxg_adjoint_shard_*): on CPU
+the two gloo ranks run its exchange with the stand-in's adjoint; on the GPU
+emulated shards, one handle each, against hxg_adjoint_device.
 """
 import os
 import socket
