@@ -17,6 +17,8 @@ Size-dependent defects (64-bit voxel indices at 512^3, the pixel walk at
 Nside 256, ray windows on 30-kpc rays) would show here and not on the small
 golden cases.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -128,3 +130,23 @@ def test_config3_inner_shells_fp32c_vs_reference(config3_inner):
     o, models, grids, ref = config3_inner
     (got,) = _gpu("fp32c", [o], models, grids)
     _compare(got, ref, TOL32, PTOL32, "config3 shells 1-2 fp32c 0.408 GHz")
+
+
+@pytest.mark.skipif(os.environ.get("HXG_FULL_PASS") != "1",
+                    reason="about 10 minutes of the reference on the host: set HXG_FULL_PASS=1")
+def test_config3_full_pass_vs_reference(torch_mod, reference):
+    """Config 3's first pass in full -- all four shells (Nside 128 to 1024,
+    to 30 kpc at 0.01 kpc) on the 512^3 grids at 30 GHz with DM and FD,
+    2.16e10 LOS samples -- in both forms against the reference run live on
+    every host core; prints the reference's write_grid time."""
+    c = W.CONFIG3
+    grids = _host_grids(torch_mod, c["grid_n"], c["seeds"])
+    o = W.config_grid(c["nside_shells"], c["r_max_kpc"], c["res_kpc"], c["freqs_ghz"])[0]
+    models = W.grid_models()
+    ref, secs = reference.write_grid(o, models, grids, nthreads=os.cpu_count())
+    print(f"reference: {secs:.1f} s on {os.cpu_count()} threads, "
+          f"{W.samples_of(o) / secs:.4g} samples/s", flush=True)
+    (g64,) = _gpu("fp64", [o], models, grids)
+    _compare(g64, ref, TOL64, PTOL64, "config3 full pass fp64 30 GHz")
+    (g32,) = _gpu("fp32c", [o], models, grids)
+    _compare(g32, ref, TOL32, PTOL32, "config3 full pass fp32c 30 GHz")
