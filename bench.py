@@ -50,17 +50,11 @@ WORKLOADS = {
                    freqs_ghz=[0.408, 1.4, 30.0], grid_n=64, seeds=(3, 4)),
 }
 # The bounded sample both arms time like for like: the first frequency pass
-# (DM + FD + synchrotron) of the workload over all its shells on 1/64 of the
-# sky -- a mask at Nside 128 keeping 192 patches of 4 x 4 pixels (every 64th
-# NESTED block of 16), replicated to the shells' Nsides (Hampisk::duplicate)
-# -- on the same grids.  The patches are spread over all twelve base faces,
-# so the sample has the workload's mix of rays and of samples inside and
-# outside the cuts (config 3: 3.4e8 LOS samples, about 1.7 s of the
-# reference on 16 host threads per step; the full pass takes 110 s), and a
-# kept patch fills whole warps of the GPU kernels.
-SUB_MASK_NSIDE = 128
-SUB_MASK_EVERY = 64
-SUB_MASK_BLOCK = 16
+# (DM + FD + synchrotron) of the workload over its innermost shell only,
+# with its own radii, Nside and sample positions, on the same grids (config
+# 3: Nside 128, 0-3.75 kpc, 7.4e7 LOS samples, about 1.5 s of the
+# reference on 16 host threads per step).
+SUB_SHELLS = 1
 
 
 def log(*a):
@@ -163,36 +157,28 @@ def make_passes(wl, nside_shells=None):
 
 
 def sub_workload(wl):
-    """Obs of the bounded sample: pass 1 of the workload, masked."""
-    o = make_passes(wl)[0]
-    o.do_mask = 1
+    """Obs of the bounded sample: pass 1 of the workload restricted to its
+    SUB_SHELLS innermost shells (the same shell radii, Nsides and radial
+    steps), output maps at the outermost of those Nsides."""
+    from hammurabix_b200 import workloads as W
+    full = make_passes(wl)[0]
+    o = W.make_obs(wl["nside_shells"][:SUB_SHELLS], wl["r_max_kpc"], wl["res_kpc"],
+                   freq_ghz=full.sync_freq / 1e9)
+    for i in range(SUB_SHELLS + 1):
+        o.radii_shell[i] = full.radii_shell[i]
     return o
 
 
-def sub_mask():
-    """The bounded sample's mask (RING map at SUB_MASK_NSIDE)."""
-    from hammurabix_b200 import workloads as W
-    return W.patch_mask(SUB_MASK_NSIDE, SUB_MASK_EVERY, SUB_MASK_BLOCK)
-
-
-def sub_samples(wl):
-    """LOS samples of the bounded sample (the kept fraction of every shell is
-    exactly 1 / SUB_MASK_EVERY: each Nside-128 pixel covers whole pixels of
-    the finer shells)."""
-    from hammurabix_b200 import workloads as W
-    return W.samples_of(sub_workload(wl)) // SUB_MASK_EVERY
-
-
 def sub_workload_text(wl):
+    from hammurabix_b200 import workloads as W
     from hammurabix_b200 import units as U
     o = sub_workload(wl)
     shells = "/".join(str(o.nside_shell[i]) for i in range(o.total_shell))
-    return (f"pass 1 ({o.sync_freq / 1e9:g} GHz with DM + FD) over all {o.total_shell} shells "
-            f"(Nside {shells}, 0-{o.radii_shell[o.total_shell] / U.kpc:g} kpc) on 1/"
-            f"{SUB_MASK_EVERY} of the sky (an Nside-{SUB_MASK_NSIDE} mask of patches of "
-            f"{SUB_MASK_BLOCK} pixels, every {SUB_MASK_EVERY}th NESTED block), same "
-            f"{wl['grid_n']}^3 grids: {sub_samples(wl)} LOS "
-            f"samples, Integrator::write_grid only")
+    what = "innermost shell" if SUB_SHELLS == 1 else f"{SUB_SHELLS} innermost shells"
+    return (f"pass 1 ({o.sync_freq / 1e9:g} GHz with DM + FD) over the workload's {what} "
+            f"(Nside {shells}, 0-{o.radii_shell[SUB_SHELLS] / U.kpc:g} kpc), "
+            f"same {wl['grid_n']}^3 grids: {W.samples_of(o)} LOS samples, "
+            f"Integrator::write_grid only")
 
 
 def cpu_baseline(wl, host_fields, steps=1):
@@ -207,13 +193,11 @@ def cpu_baseline(wl, host_fields, steps=1):
     o = sub_workload(wl)
     grids = W.grids_dict(wl["grid_n"], *host_fields)
     m = W.grid_models()
-    mask = sub_mask()
     times = []
     for _ in range(steps):
-        _, secs = ref.write_grid(o, m, grids, mask=mask, mask_nside=SUB_MASK_NSIDE,
-                                 nthreads=threads)
+        _, secs = ref.write_grid(o, m, grids, nthreads=threads)
         times.append(secs)
-    return {"samples": sub_samples(wl), "seconds": times, "threads": threads,
+    return {"samples": W.samples_of(o), "seconds": times, "threads": threads,
             "sample": sub_workload_text(wl)}
 
 
@@ -628,10 +612,10 @@ def main():
     if args.sub_steps > 0 and not shard:
         osub = sub_workload(wl)
         nsub = abi.npix(osub.nside_dm)
-        sub = {"sample": sub_workload_text(wl), "samples": sub_samples(wl)}
+        sub = {"sample": sub_workload_text(wl), "samples": W.samples_of(osub),
+               "valid_samples": sum(W.valid_samples(osub))}
         for prec in ("fp64", "fp32c"):
             ig_ = make_integ(prec)
-            ig_.set_mask(SUB_MASK_NSIDE, sub_mask())
             m5 = [torch.zeros(nsub, dtype=torch.float64, device=dev) for _ in range(5)]
             ig_.write_grid_device(osub, *m5)
             ev0 = torch.cuda.Event(enable_timing=True)

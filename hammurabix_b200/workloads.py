@@ -104,54 +104,6 @@ def frequency_passes(obs_template, freqs_ghz):
     return passes
 
 
-def _compress_bits(v):
-    """The even bits of v packed together (HEALPix NESTED x or y index)."""
-    v = v & 0x5555555555555555
-    v = (v | (v >> 1)) & 0x3333333333333333
-    v = (v | (v >> 2)) & 0x0F0F0F0F0F0F0F0F
-    v = (v | (v >> 4)) & 0x00FF00FF00FF00FF
-    v = (v | (v >> 8)) & 0x0000FFFF0000FFFF
-    v = (v | (v >> 16)) & 0x00000000FFFFFFFF
-    return v
-
-
-def nest2ring(nside, nest):
-    """RING index of NESTED pixels at Nside `nside` (the HEALPix face / x-y
-    decomposition, Gorski et al. 2005): numpy int64 arrays."""
-    nest = np.asarray(nest, dtype=np.int64)
-    npface = nside * nside
-    npix = 12 * npface
-    face = nest // npface
-    ipf = nest % npface
-    ix = _compress_bits(ipf)
-    iy = _compress_bits(ipf >> 1)
-    jrll = np.array([2, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4], dtype=np.int64)
-    jpll = np.array([1, 3, 5, 7, 0, 2, 4, 6, 1, 3, 5, 7], dtype=np.int64)
-    nl4 = 4 * nside
-    jr = jrll[face] * nside - ix - iy - 1
-    north, south = jr < nside, jr > 3 * nside
-    nr = np.where(north, jr, np.where(south, nl4 - jr, nside))
-    kshift = np.where(north | south, 0, (jr - nside) & 1)
-    ncap = 2 * nside * (nside - 1)
-    n_before = np.where(north, 2 * nr * (nr - 1),
-                        np.where(south, npix - 2 * (nr + 1) * nr, ncap + (jr - nside) * nl4))
-    jp = (jpll[face] * nr + ix - iy + 1 + kshift) // 2
-    jp = np.where(jp > nl4, jp - nl4, jp)
-    jp = np.where(jp < 1, jp + nl4, jp)
-    return n_before + jp - 1
-
-
-def patch_mask(nside, every, block):
-    """RING mask at `nside` keeping 1/`every` of the sky in compact patches:
-    the NESTED blocks of `block` pixels whose block index is a multiple of
-    `every`, spread over all twelve base faces."""
-    nest = np.arange(12 * nside * nside, dtype=np.int64)
-    keep = (nest // block) % every == 0
-    m = np.zeros(nest.size)
-    m[nest2ring(nside, nest[keep])] = 1.0
-    return m
-
-
 def grid_desc(n, box_kpc=BOX_KPC):
     g = abi.GridDesc()
     g.nx = g.ny = g.nz = n

@@ -88,22 +88,3 @@ def test_no_device_fails_loudly():
     assert lib.hxg_pix2ang(2, 48, _lib.dptr(th), _lib.dptr(ph)) == abi.HXG_ERR_NO_DEVICE
     with pytest.raises(_lib.HxgError):
         I.Integrator("fp64")
-
-
-def test_nest2ring_and_patch_masks():
-    """workloads.nest2ring (the bench's sky-patch masks): a permutation of
-    the RING indices, and the NESTED children 4p..4p+3 of a pixel are the
-    pixels the library's mask upgrade (Hampisk::duplicate) sets."""
-    from hammurabix_b200 import workloads as W
-    for ns in (1, 2, 4, 8, 32):
-        r = W.nest2ring(ns, np.arange(12 * ns * ns))
-        assert np.array_equal(np.sort(r), np.arange(12 * ns * ns)), ns
-    rng = np.random.default_rng(0)
-    for p in rng.integers(0, 768, 24):
-        m = np.zeros(768)
-        m[W.nest2ring(8, [p])] = 1.0
-        want = np.zeros(3072)
-        want[W.nest2ring(16, np.arange(4 * p, 4 * p + 4))] = 1.0
-        assert np.array_equal(I.mask_duplicate(8, m, 16), want), p
-    m = W.patch_mask(128, 64, 16)
-    assert m.sum() * 64 == m.size
