@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the B200 line-of-sight integrator.
 
-Workload (default): Nside 128/256/512/1024 over 4 shells
+Workload (default, "config3"): Nside 128/256/512/1024 over 4 shells
 to 30 kpc with 0.01 kpc radial steps (21.6 G LOS samples per frequency),
 512^3 FP32 random-field grids (B_rnd 3 components + lognormal n_e) on a
 40 x 40 x 10 kpc box plus the analytic spiral B_reg and CRE_ana, three
