@@ -687,7 +687,9 @@ shell_fp32c_kernel(const ShellLaunch P) {
 // HXG_FP32C_MULTI_THREADS x HXG_FP32C_MULTI_MIN_BLOCKS: the per-pass Q/U
 // sums and phase constants take registers).
 template <int NG, bool kExt, int NF, bool kFast>
-__global__ void __launch_bounds__(HXG_FP32C_MULTI_THREADS, HXG_FP32C_MULTI_MIN_BLOCKS)
+__global__ void __launch_bounds__(HXG_FP32C_MULTI_THREADS,
+                                  kFast ? HXG_FP32C_MULTI_MIN_BLOCKS_FAST
+                                        : HXG_FP32C_MULTI_MIN_BLOCKS)
 shell_fp32c_multi_kernel(const ShellLaunch P, const FreqSet<NF> Fq) {
   fp32c_tile<NG, kExt, NF, kFast>(P, Fq, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
                            threadIdx.x & 31);

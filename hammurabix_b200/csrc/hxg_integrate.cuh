@@ -113,10 +113,15 @@ __host__ __device__ inline bool fast_models(const ShellLaunch &P) {
 // the resident blocks per SM its register budget is cut for.  128 x 5
 // (96 registers) keeps 20 warps per SM; for the general instantiation it ran
 // config 3 in 91.3 ms against 92.8 ms at 256 x 2 (128 registers) and
-// 97.2 ms at 128 x 6 (80 registers, more spills); the kFast instantiation
-// needs no spill at 96 registers and is within 2 % at 128 x 4 and 128 x 6.
+// 97.2 ms at 128 x 6 (80 registers, more spills).  The kFast instantiation
+// runs 128 x 7 (72 registers, 28 warps): config 3's fused step 59.1 ms
+// against 59.5 ms at 128 x 5, 59.7 ms at 128 x 6, 61.3 ms at 128 x 8 and
+// 68.5 ms at 128 x 9 (the spills grow with each step).
 #ifndef HXG_FP32C_MULTI_THREADS
 #define HXG_FP32C_MULTI_THREADS 128
+#endif
+#ifndef HXG_FP32C_MULTI_MIN_BLOCKS_FAST
+#define HXG_FP32C_MULTI_MIN_BLOCKS_FAST 7
 #endif
 #ifndef HXG_FP32C_MULTI_MIN_BLOCKS
 #define HXG_FP32C_MULTI_MIN_BLOCKS 5
