@@ -73,8 +73,9 @@ __device__ __forceinline__ void batch_multi_body(const BatchLevelMulti<NF> &B) {
 }
 
 // Launch shape of the fused batch kernel (threads per block, resident
-// blocks per SM its register allocation must allow).  256 x 2 ran config 5
-// in 1149 ms against 1214-1216 ms at 128 x 5 and 128 x 6.
+// blocks per SM its register allocation must allow).  256 x 2 (128
+// registers) runs config 5 in 927 ms against 943 ms at 128 x 5, 968 ms at
+// 256 x 3 and 988 ms at 128 x 7 (the smaller budgets spill 300-460 bytes).
 #ifndef HXG_BATCH_MULTI_THREADS
 #define HXG_BATCH_MULTI_THREADS 256
 #endif
